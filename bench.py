@@ -1,0 +1,301 @@
+#!/usr/bin/env python
+"""IISPH time-step benchmark on the 1,000,000-particle dam break (one B200).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one IISPH.step() (IISPH.py:1002-1371): cell sort, neighbour build
+and advection prediction, the relaxed-Jacobi solve to 0.1 % average density
+error, kick/drift and CFL.  The workload is the dam break of 100^3 fluid
+particles at 0.01 m spacing with +-5e-5 m seeded jitter in a 2 x 1 x 1 m box
+with 2 boundary layers (206,464 boundary particles), 1024-sample kernel tables,
+g = 9.81, dt = 5e-4 s.  Inputs are synthetic (seeded); the state and neighbour
+lists (~0.5 GB) exceed the 126 MB L2, so no flush is needed between steps.
+
+Prints one JSON line (rank 0).  With torchrun (N > 1) every rank runs an
+independent replica of the scene: the single-scene step does not shard
+(replicas only), so there is no data-path collective; timing is the max over
+ranks and `value` counts the steps of all ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "IISPH steps/s at 1M particles, 0.1% density err; learned warm-start vs plain"
+PRESET = "dam_break_1m"
+KERNELS_PER_STEP = 8  # cell_keys, scan_part, scan_final, scatter, cell_sort, gather, build, jacobi
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_cpu_reference(budget_s: float, max_steps: int, nthreads: int = 0):
+    """The reference algorithm (CPU oracle, FP32, OpenMP) on the same scene."""
+    from oracle import oracle
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+    from warpsph_b200.tables import kernel_tables
+
+    oracle.build()
+    params = preset_params(PRESET)
+    scene = preset_scene(PRESET)
+    op = oracle.reference_params(diameter=params.diameter, gravity=params.gravity, w_size=1024, g_size=1024)
+    tabs = kernel_tables(params)
+    nt = nthreads or oracle.max_threads()
+    psi = oracle.boundary_psi(op, scene.boundary_x, tables=tabs, nthreads=nt)
+    x, v = scene.fluid_x.copy(), scene.fluid_v.copy()
+    dt, inv_dt = params.dt_max, 1.0 / params.dt_max
+    steps, t_total, iters = 0, 0.0, []
+    while steps < max_steps and (steps == 0 or t_total < budget_s):
+        t0 = time.perf_counter()
+        r = oracle.step(op, x, v, scene.boundary_x, None, psi, dt, inv_dt, tables=tabs, export=False,
+                        nthreads=nt)
+        t_total += time.perf_counter() - t0
+        x, v, dt, inv_dt = r["x"], r["v"], r["dt_next"], r["inv_dt_next"]
+        iters.append(r["iterations"])
+        steps += 1
+    return {"value": steps / t_total, "unit": "steps/s", "cores": nt, "kind": "port",
+            "sample": f"first {steps} steps of the 1M-particle dam break from its initial state "
+                      f"(FP32 oracle, {nt} OpenMP threads), iterations {iters}"}
+
+
+def bench_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    base = run_cpu_reference(budget_s=150.0, max_steps=max(1, args.steps))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": base["value"], "unit": "steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 / base["value"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "dam break, 1,000,000 fluid + 206,464 boundary particles, tol 0.1% avg density err",
+                   "preset": PRESET},
+        "cpu_baseline": base,
+        "e2e": {"value": base["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def bench_ours(args):
+    import ctypes
+
+    import torch
+
+    from warpsph_b200 import _lib
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+    from warpsph_b200.solver import IISPH
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    params = preset_params(PRESET, device=local)
+    scene = preset_scene(PRESET)
+    sol = IISPH(stage_path=None, params=params, scene=scene)
+    L, ctx = sol._lib, sol._ctx
+    stream = torch.cuda.ExternalStream(L.sph_stream(ctx), device=torch.device("cuda", local))
+    n = scene.n
+
+    sol.steps(args.warmup)  # also captures the step graph
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    _lib.check(ctx, L.sph_launch_steps(ctx, args.steps))
+    ev1.record(stream)
+    ev1.synchronize()
+    clock = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    hist = sol.stats_history(args.steps)
+    flags = 0
+    for h in hist:
+        flags |= h["flags"]
+    if flags & (_lib.SPH_F_TIMEOUT | _lib.SPH_F_NONFINITE | _lib.SPH_F_FF_OVERFLOW | _lib.SPH_F_FB_OVERFLOW):
+        raise RuntimeError(f"step flags {flags:#x} in the timed region")
+    iters = [h["iterations"] for h in hist]
+    errs = [h["avg_err"] for h in hist]
+    pairs = [h["n_ff_pairs"] for h in hist]
+    ms_t = torch.tensor([ms], device="cuda")
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * args.steps / (ms_max / 1000.0)
+
+    # dominant kernel (the persistent Jacobi solve): per-launch CUDA-event time
+    kt = min(args.steps, 20)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(kt)]
+    evf = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(kt)]
+    for a, b in zip(evs, evf):
+        b[0].record(stream)
+        _lib.check(ctx, L.sph_launch_phase(ctx, 0))
+        b[1].record(stream)
+        a[0].record(stream)
+        _lib.check(ctx, L.sph_launch_phase(ctx, 1))
+        a[1].record(stream)
+    torch.cuda.synchronize()
+    hk = sol.stats_history(kt)
+    t_jac = [a.elapsed_time(b) for a, b in evs]
+    t_front = [a.elapsed_time(b) for a, b in evf]
+    bytes_launch = [h["iterations"] * (100.0 * n + 8.0 * h["n_ff_pairs"]) + 112.0 * n for h in hk]
+    achieved = sum(bytes_launch) / (sum(t_jac) / 1000.0) / 1e9
+    peak, peak_kind = _peaks()
+    traffic = None
+    tf = ROOT / "profiles" / "jacobi_traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+
+    # end to end through the C ABI with host buffers: every step uploads its
+    # input state (x, v) from pinned memory and reads back x, v, p
+    e2e_steps = min(args.steps, 10)
+    hx = torch.from_numpy(scene.fluid_x.copy()).pin_memory()
+    hv = torch.from_numpy(scene.fluid_v.copy()).pin_memory()
+    hp = torch.zeros(n, dtype=torch.float32).pin_memory()
+    sol.set_dt(params.dt_max)
+    st = _lib.SphStepStats()
+    vp = ctypes.c_void_p
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        _lib.check(ctx, L.sph_set_fluid(ctx, vp(hx.data_ptr()), vp(hv.data_ptr()), n))
+        _lib.check(ctx, L.sph_step(ctx, ctypes.byref(st)))
+        _lib.check(ctx, L.sph_get_fluid(ctx, vp(hx.data_ptr()), vp(hv.data_ptr()), vp(hp.data_ptr()), None, None))
+    e2e_s = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_s], device="cuda")
+    if dist:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * e2e_steps / float(e2e_t.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = run_cpu_reference(budget_s=20.0, max_steps=3)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "dam break, 1,000,000 fluid + 206,464 boundary particles, tol 0.1% avg density err",
+                       "preset": PRESET, "warm_start": params.warm_start, "parallelism": f"replicas{world}",
+                       "l2": "working set > 126 MB L2 (no flush needed)"},
+            "particle_updates_per_s": value * n,
+            "jacobi_iterations_mean": float(np.mean(iters)), "avg_err_max": float(np.max(errs)),
+            "n_ff_pairs_mean": float(np.mean(pairs)),
+            "phase_ms": {"front": float(np.mean(t_front)), "solve": float(np.mean(t_jac))},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_jacobi (persistent solve + kick/drift)"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 24 * n,
+                    "d2h_bytes_per_step": 28 * n + 80},
+            "gpu_launches": KERNELS_PER_STEP * args.steps,
+            "clocks": clock,
+        }
+        print(json.dumps(line), flush=True)
+    sol.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        bench_reference(args)
+    else:
+        bench_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,172 @@
+/* wpsph.h — C ABI of libwpsph.so, the B200 (sm_100a) IISPH time step.
+ *
+ * The reference (Mo-ZheHan/WarpSPH) has no native layer: its Python class
+ * wp_sph.solver.IISPH (wp_sph/solver/IISPH.py:736) drives Warp kernels.  These
+ * entry points are what that class binds through ctypes in place of its Warp
+ * arrays and launches; each declaration names the reference code it replaces.
+ *
+ * Conventions
+ *   - Every int-returning call returns SPH_OK (0) or a negative SPH_E_* code;
+ *     sph_last_error() describes the last failure.  Nothing throws or exits.
+ *   - Host buffers are caller-owned and copied; device buffers are owned by the
+ *     context.  Arrays are in the caller's ORIGINAL particle order; the cell-
+ *     sorted order the kernels use internally is never exposed.
+ *   - One context = one CUDA device + one CUDA stream.  A context is not
+ *     thread-safe; distinct contexts are independent.
+ *   - float3 arrays are packed xyz, 3 floats per particle.
+ */
+#ifndef WPSPH_H
+#define WPSPH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WPSPH_ABI_VERSION 1
+
+#define SPH_OK 0
+#define SPH_E_INVALID -1   /* bad argument or call order */
+#define SPH_E_CUDA -2      /* CUDA runtime error */
+#define SPH_E_CAPACITY -3  /* neighbour capacity exceeded (raise max_ff / max_fb) */
+#define SPH_E_NONFINITE -4 /* NaN/Inf in pressure or velocity */
+#define SPH_E_TIMEOUT -5   /* a bounded grid-wide wait expired */
+#define SPH_E_NOMEM -6     /* device allocation failed */
+
+/* SphStepStats.flags bits */
+#define SPH_F_FF_OVERFLOW 0x1
+#define SPH_F_FB_OVERFLOW 0x2
+#define SPH_F_NONFINITE 0x4
+#define SPH_F_TIMEOUT 0x8
+#define SPH_F_NOT_CONVERGED 0x10 /* hit the iteration cap (IISPH.py:1202-1207: a print) */
+
+/* Warm-start modes for the pressure solve (IISPH.py:166-174). */
+#define SPH_WARM_ZERO 0 /* p <- 0, the reference's behaviour (IISPH.py:173) */
+#define SPH_WARM_HALF 1 /* p <- 0.5 p_prev (the variant at IISPH.py:174) */
+#define SPH_WARM_MLP 2  /* p <- learned per-particle MLP prediction */
+
+typedef struct SphParams {
+  double spacing;    /* DIAMETER (wp_sph/main.py:26) */
+  double h;          /* SMOOTHING_LENGTH = 2*DIAMETER (main.py:57) */
+  double rho0;       /* RHO_0 (main.py:30) */
+  double gravity;    /* GRAVITY (main.py:25); acts along -y */
+  double omega;      /* OMEGA, relaxed-Jacobi weight (main.py:27) */
+  double eta;        /* ETA, average density error tolerance (main.py:28) */
+  double inv_small;  /* INV_SMALL (main.py:29) */
+  double vis_mu;     /* VIS_MU (main.py:61) */
+  double fluid_mass; /* FLUID_MASS = RHO_0*DIAMETER^3 (main.py:59) */
+  double sigma;      /* SIGMA = 8/(pi h^3) (main.py:60) */
+  double dt_max;     /* TIME_STEP_MAX = 0.05*DIAMETER (main.py:58) */
+  double cfl_len;    /* 0.4*DIAMETER (IISPH.py:1369) */
+  double dt0;        /* first step's dt (IISPH.py:747) */
+  double domain_min[3], domain_max[3]; /* neighbour-grid extent; zero extent = fit to particles */
+  int32_t w_table_size;  /* W_SIZE (sph_funcs.py:43) */
+  int32_t g_table_size;  /* GRAD_W_SIZE (sph_funcs.py:44) */
+  int32_t min_iter;      /* 2  (IISPH.py:1201) */
+  int32_t max_loop;      /* 100 (IISPH.py:1202) */
+  int32_t fixed_iters;   /* -1 = converge; >= 1 = exactly this many iterations */
+  int32_t warm_start;    /* SPH_WARM_* */
+  int32_t max_ff;        /* fluid-fluid neighbour capacity per particle */
+  int32_t max_fb;        /* fluid-boundary neighbour capacity per particle */
+  int32_t keep_fb_lists; /* also store fluid-boundary lists (for sph_get_neighbors) */
+  int32_t use_graph;     /* replay the step as a CUDA graph */
+  int32_t device;        /* CUDA device ordinal */
+  int32_t block_size;    /* threads per block for particle kernels (0 = auto) */
+  int32_t timeout_ms;    /* bound on every grid-wide wait */
+  int32_t reserved[5];
+} SphParams;
+
+typedef struct SphStepStats {
+  int32_t iterations; /* Jacobi iterations executed (IISPH.py:1200-1296 `loop`) */
+  int32_t flags;      /* SPH_F_* */
+  double avg_err;     /* average_rho_error (IISPH.py:1489-1494), FP64 reduction */
+  double v_max;       /* max |v| after the kick (IISPH.py:688) */
+  double dt;          /* dt used by this step */
+  double dt_next;     /* CFL dt for the next step (IISPH.py:1368-1370) */
+  double sim_time;    /* sim_time after this step (IISPH.py:1367) */
+  int64_t n_ff_pairs; /* sum of fluid-fluid neighbour counts */
+  int64_t n_fb_pairs; /* sum of fluid-boundary neighbour counts */
+  int32_t max_ff_count, max_fb_count;
+  int64_t step_index;
+} SphStepStats;
+
+typedef struct SphCtx SphCtx;
+
+/* Reference defaults: the constants of wp_sph/main.py:25-61 and sph_funcs.py:43-44. */
+int sph_params_default(SphParams* p);
+
+/* Replaces IISPH.__init__'s array allocation and hash-grid creation (IISPH.py:770-805). */
+int sph_create(const SphParams* params, SphCtx** out);
+void sph_destroy(SphCtx* ctx);
+const char* sph_last_error(const SphCtx* ctx);
+
+/* Kernel tables (sph_funcs.py:47-86).  Optional: without it the library builds
+ * the tables itself from params (FP64 then float32, as sph_funcs.py does). */
+int sph_set_tables(SphCtx* ctx, const float* w_table, int32_t w_size, const float* g_table, int32_t g_size);
+
+/* The tables sph_create builds when none are set, written to caller buffers of
+ * params->w_table_size and params->g_table_size floats.  Host only (no GPU). */
+int sph_build_tables(const SphParams* params, float* w_table, float* g_table);
+
+/* Boundary particles (IISPH.py:990-991) and their volume psi, computed once
+ * (compute_boundary_density, IISPH.py:23-49, launched at IISPH.py:811-821). */
+int sph_set_boundary(SphCtx* ctx, const float* xb3, const float* vb3, int64_t nb);
+
+/* Fluid particles (IISPH.py:993-994) with velocities (NULL = zero). */
+int sph_set_fluid(SphCtx* ctx, const float* x3, const float* v3, int64_t n);
+
+/* Pressure carried into the next step's warm start (SPH_WARM_HALF / SPH_WARM_MLP). */
+int sph_set_pressure(SphCtx* ctx, const float* p, int64_t n);
+
+/* One time step: IISPH.step() (IISPH.py:1002-1371).  Blocks until the step's
+ * statistics are on the host when out != NULL. */
+int sph_step(SphCtx* ctx, SphStepStats* out);
+
+/* nsteps time steps back to back with one host synchronisation; per-step stats
+ * (up to 4096 most recent) are then available from sph_get_stats_history. */
+int sph_steps(SphCtx* ctx, int32_t nsteps, SphStepStats* last);
+int sph_get_stats_history(SphCtx* ctx, SphStepStats* out, int32_t count);
+
+/* Asynchronous forms for callers that time with CUDA events on sph_stream():
+ * enqueue nsteps steps, or one phase of a step (0 = cell sort + neighbour
+ * build + advection prediction, 1 = pressure solve + kick/drift/CFL), with no
+ * host synchronisation.  Flags surface at the next sph_get_stats/sph_step. */
+int sph_launch_steps(SphCtx* ctx, int32_t nsteps);
+int sph_launch_phase(SphCtx* ctx, int32_t phase);
+
+/* IISPH.neighbor_search() (IISPH.py:1408-1482): cell sort + neighbour build +
+ * density for the current state, without advancing time. */
+int sph_neighbor_search(SphCtx* ctx);
+
+/* Read back state in original order; any pointer may be NULL.
+ * x/v/p/rho/rho_adv mirror the IISPH attributes of the same names (IISPH.py:783-788). */
+int sph_get_fluid(SphCtx* ctx, float* x3, float* v3, float* p, float* rho, float* rho_adv);
+/* Intermediate terms of the last step: term_d_ii, term_a_ii, sum_d_ij_p_j, v_adv
+ * (IISPH.py:784, 792-797), and term_Ap_i of the last pass. */
+int sph_get_terms(SphCtx* ctx, float* d_ii3, float* a_ii, float* s3, float* v_adv3, float* Ap);
+/* boundary_x and boundary_phi (IISPH.py:789, 990) in original boundary order. */
+int sph_get_boundary(SphCtx* ctx, float* xb3, float* psi);
+/* Neighbour sets of the last build in original ids, CSR per fluid particle,
+ * ids ascending (ff_neighbor_* / fs_neighbor_*, IISPH.py:798-805).
+ * fb lists need params.keep_fb_lists. */
+int sph_get_neighbors(SphCtx* ctx, int64_t* ff_off, int32_t* ff_idx, int64_t ff_cap,
+                      int64_t* fb_off, int32_t* fb_idx, int64_t fb_cap);
+
+int sph_get_stats(SphCtx* ctx, SphStepStats* out);
+/* Override dt / 1/dt for the next step (the reference's self.dt, self.inv_dt). */
+int sph_set_dt(SphCtx* ctx, double dt, double inv_dt);
+/* ABI self-description, needs no GPU: out[0] = WPSPH_ABI_VERSION,
+ * out[1] = sizeof(SphParams), out[2] = sizeof(SphStepStats). */
+int sph_abi_info(int32_t* out, int32_t count);
+int64_t sph_num_fluid(const SphCtx* ctx);
+int64_t sph_num_boundary(const SphCtx* ctx);
+/* The context's cudaStream_t, for event timing by the caller. */
+void* sph_stream(SphCtx* ctx);
+int sph_synchronize(SphCtx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WPSPH_H */

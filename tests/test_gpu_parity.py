@@ -1,0 +1,256 @@
+"""GPU parity: libwpsph (through its C ABI, via the drop-in IISPH class) against
+the reference's golden vectors and the CPU oracle on identical input states.
+
+Bars (from the hot-path contract):
+  * neighbour sets bit-exact (integer work);
+  * per-step density, pressure, positions within 1e-4 relative (norm-wise:
+    max |gpu - ref| / max |ref|);
+  * Jacobi iteration count within +-1.
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import csr_equal, load_golden, normrel
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-4
+
+
+def _solver(params, scene):
+    from warpsph_b200.solver import IISPH
+
+    return IISPH(stage_path=None, params=params, scene=scene)
+
+
+def _golden_params(meta, **kw):
+    from warpsph_b200.params import SolverParams
+
+    return SolverParams(diameter=meta["diameter"], gravity=meta["gravity"], w_table_size=meta["w_size"],
+                        g_table_size=meta["g_size"], keep_fb_lists=True, **kw)
+
+
+def _golden_scene(G, s):
+    from warpsph_b200.scenes import Scene
+
+    bx = G["boundary_x"]
+    return Scene(G[f"s{s}_x_in"], G[f"s{s}_v_in"], bx, len(bx), (0, 0, 0))
+
+
+@pytest.mark.parametrize("name", ["ref_lattice", "dam_jitter", "compressed"])
+def test_golden_steps(name):
+    G, meta = load_golden(name)
+    sol = _solver(_golden_params(meta), _golden_scene(G, 0))
+    assert normrel(sol.boundary_phi.numpy(), G["boundary_phi"]) < 1e-5
+    for s in range(int(G["steps"])):
+        pre = f"s{s}_"
+        sol.set_state(G[pre + "x_in"], G[pre + "v_in"])
+        sol.set_dt(float(G[pre + "dt_in"]), float(G[pre + "inv_dt_in"]))
+        sol.step()
+        nb = sol.get_neighbors(with_boundary=True)
+        assert csr_equal(nb["ff_off"], nb["ff_idx"], G[pre + "ff_off"], G[pre + "ff_idx"]), f"ff sets, step {s}"
+        assert csr_equal(nb["fb_off"], nb["fb_idx"], G[pre + "fb_off"], G[pre + "fb_idx"]), f"fb sets, step {s}"
+        assert normrel(sol.rho.numpy(), G[pre + "rho"]) < RTOL
+        assert normrel(sol.rho_adv.numpy(), G[pre + "rho_adv"]) < RTOL
+        assert normrel(sol.v_adv.numpy(), G[pre + "v_adv"]) < RTOL
+        assert normrel(sol.term_d_ii.numpy(), G[pre + "d_ii"]) < RTOL
+        assert normrel(sol.term_a_ii.numpy(), G[pre + "a_ii"]) < RTOL
+        it_ref = int(G[pre + "iterations"])
+        it = sol.last_stats["iterations"]
+        assert abs(it - it_ref) <= 1, (it, it_ref)
+        if it == it_ref:
+            assert normrel(sol.p.numpy(), G[pre + "p"]) < RTOL
+            assert normrel(sol.sum_d_ij_p_j.numpy(), G[pre + "s"]) < RTOL
+            assert normrel(sol.v.numpy(), G[pre + "v_out"]) < RTOL
+            assert normrel(sol.x.numpy(), G[pre + "x_out"]) < 1e-6
+        assert abs(sol.dt - float(G[pre + "dt_out"])) <= 1e-4 * float(G[pre + "dt_out"])
+    sol.close()
+
+
+@pytest.mark.parametrize("name", ["dam_jitter", "compressed"])
+def test_golden_fixed_iterations(name):
+    """Pressure after exactly the reference's iteration count, even where the
+    convergence test would stop one iteration apart."""
+    G, meta = load_golden(name)
+    for s in range(int(G["steps"])):
+        pre = f"s{s}_"
+        sol = _solver(_golden_params(meta, fixed_iters=int(G[pre + "iterations"])), _golden_scene(G, s))
+        sol.set_dt(float(G[pre + "dt_in"]), float(G[pre + "inv_dt_in"]))
+        sol.step()
+        assert sol.last_stats["iterations"] == int(G[pre + "iterations"])
+        assert normrel(sol.p.numpy(), G[pre + "p"]) < RTOL
+        assert normrel(sol.term_Ap_i.numpy(), G[pre + "Ap"]) < RTOL
+        assert normrel(sol.v.numpy(), G[pre + "v_out"]) < RTOL
+        sol.close()
+
+
+def _oracle_step(oracle, params, x, v, bx, psi, dt, inv_dt, precision="f32", **kw):
+    from warpsph_b200.tables import kernel_tables
+
+    op = oracle.reference_params(diameter=params.diameter, gravity=params.gravity, w_size=params.w_table_size,
+                                 g_size=params.g_table_size)
+    tabs = kernel_tables(params)
+    if precision == "f64":
+        tabs = oracle.kernel_tables(op, np.float64)
+    return oracle.step(op, x, v, bx, None, psi, dt, inv_dt, tables=tabs, precision=precision, **kw)
+
+
+def test_dam_break_8k_vs_oracle(oracle):
+    """The 8,000-particle dam break: one step from the initial state and one
+    from a state 30 GPU steps later, GPU vs the FP32 oracle (and FP64 truth)."""
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+
+    params = preset_params("dam_break_8k", keep_fb_lists=True)
+    scene = preset_scene("dam_break_8k")
+    sol = _solver(params, scene)
+    psi = sol.boundary_phi.numpy()
+    op = oracle.reference_params(diameter=params.diameter, gravity=params.gravity, w_size=1024, g_size=1024)
+    from warpsph_b200.tables import kernel_tables
+
+    assert normrel(psi, oracle.boundary_psi(op, scene.boundary_x, tables=kernel_tables(params))) < 1e-5
+    for warm in (0, 30):
+        if warm:
+            sol.steps(warm)
+        x, v = sol.x.numpy(), sol.v.numpy()
+        dt = sol.dt
+        ref = _oracle_step(oracle, params, x, v, scene.boundary_x, psi, dt, 1.0 / dt)
+        truth = _oracle_step(oracle, params, x, v, scene.boundary_x, psi, dt, 1.0 / dt, precision="f64")
+        sol.set_state(x, v)
+        sol.set_dt(dt, 1.0 / dt)
+        sol.step()
+        nb = sol.get_neighbors(with_boundary=True)
+        assert csr_equal(nb["ff_off"], nb["ff_idx"], ref["ff_off"], ref["ff_idx"])
+        assert csr_equal(nb["fb_off"], nb["fb_idx"], ref["fb_off"], ref["fb_idx"])
+        assert normrel(sol.rho.numpy(), ref["rho"]) < RTOL
+        assert normrel(sol.rho_adv.numpy(), ref["rho_adv"]) < RTOL
+        assert normrel(sol.term_a_ii.numpy(), ref["a_ii"]) < RTOL
+        assert abs(sol.last_stats["iterations"] - ref["iterations"]) <= 1
+        if sol.last_stats["iterations"] == ref["iterations"]:
+            assert normrel(sol.p.numpy(), ref["p"]) < RTOL
+            assert normrel(sol.v.numpy(), ref["v"]) < RTOL
+            assert normrel(sol.x.numpy(), ref["x"]) < 1e-6
+            # error against FP64 truth stays at the FP32 mirror's level
+            e_gpu = normrel(sol.rho.numpy(), truth["rho"])
+            e_f32 = normrel(ref["rho"], truth["rho"])
+            assert e_gpu < max(10 * e_f32, 1e-6)
+    sol.close()
+
+
+def test_warm_start_half_vs_oracle(oracle):
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+
+    params = preset_params("dam_break_8k", warm_start="half")
+    scene = preset_scene("dam_break_8k")
+    sol = _solver(params, scene)
+    sol.steps(20)
+    x, v, p = sol.x.numpy(), sol.v.numpy(), sol.p.numpy()
+    psi = sol.boundary_phi.numpy()
+    ref = _oracle_step(oracle, params, x, v, scene.boundary_x, psi, sol.dt, 1.0 / sol.dt, p=p, warm_start=1,
+                       fixed_iters=4)
+    sol2 = _solver(params.replace(fixed_iters=4), scene)
+    sol2.set_state(x, v)
+    sol2.set_pressure(p)
+    sol2.set_dt(sol.dt, 1.0 / sol.dt)
+    sol2.step()
+    assert normrel(sol2.p.numpy(), ref["p"]) < RTOL
+    assert normrel(sol2.v.numpy(), ref["v"]) < RTOL
+    sol.close()
+    sol2.close()
+
+
+def test_deterministic_and_graph_equivalent():
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+
+    scene = preset_scene("dam_break_8k")
+    outs = []
+    for use_graph in (True, True, False):
+        sol = _solver(preset_params("dam_break_8k", use_graph=use_graph), scene)
+        sol.steps(10)
+        outs.append((sol.x.numpy(), sol.v.numpy(), sol.p.numpy()))
+        sol.close()
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a, b)
+    for a, b in zip(outs[0], outs[2]):
+        assert np.array_equal(a, b)
+
+
+def test_capacity_auto_grow():
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+
+    scene = preset_scene("dam_break_8k")
+    a = _solver(preset_params("dam_break_8k"), scene)
+    b = _solver(preset_params("dam_break_8k", max_ff=4, max_fb=4, keep_fb_lists=True), scene)
+    a.steps(3)
+    b.steps(3)
+    assert np.array_equal(a.x.numpy(), b.x.numpy())
+    assert np.array_equal(a.p.numpy(), b.p.numpy())
+    a.close()
+    b.close()
+
+
+def test_empty_fluid_and_isolated_particle(oracle):
+    from warpsph_b200.params import SolverParams
+    from warpsph_b200.scenes import Scene, box_boundary
+
+    params = SolverParams(diameter=0.05)
+    bx = box_boundary((0.5, 0.5, 0.5), 0.05, 2).astype(np.float32)
+    empty = Scene(np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32), bx, len(bx), (0.5, 0.5, 0.5))
+    sol = _solver(params, empty)
+    sol.step()
+    assert sol.last_stats["iterations"] == 2 and sol.last_stats["avg_err"] == 0.0
+    sol.close()
+    # one particle far from everything: a_ii = 0 takes the sign(0) * INV_SMALL branch
+    x = np.array([[0.25, 0.3, 0.25]], np.float32)
+    lone = Scene(x, np.zeros_like(x), bx, len(bx), (0.5, 0.5, 0.5))
+    sol = _solver(params, lone)
+    sol.step()
+    psi = sol.boundary_phi.numpy()
+    ref = _oracle_step(oracle, params, x, np.zeros_like(x), bx, psi, params.dt_max, 1 / params.dt_max)
+    assert normrel(sol.p.numpy(), ref["p"]) < RTOL
+    assert ref["p"][0] > 1e8
+    assert normrel(sol.v.numpy(), ref["v"]) < RTOL
+    sol.close()
+
+
+def test_particles_outside_grid_domain(oracle):
+    """Particles far outside the grid are clamped into edge cells; their
+    neighbour sets must still be exact."""
+    from warpsph_b200.params import SolverParams
+    from warpsph_b200.scenes import dam_break
+
+    params = SolverParams(diameter=0.02, w_table_size=1024, g_table_size=1024, keep_fb_lists=True,
+                          domain_min=(0.0, 0.0, 0.0), domain_max=(0.2, 0.2, 0.2))
+    sc = dam_break(fluid=(8, 8, 8), spacing=0.02, box=(0.4, 0.3, 0.3), jitter=1e-4, layers=2, seed=3)
+    x = sc.fluid_x.copy()
+    x[:64] += np.array([0.5, 0.0, 0.0], np.float32)   # beyond the grid's x extent
+    x[64:80] -= np.array([0.0, 0.0, 0.3], np.float32)  # beyond the grid's low z side
+    sc.fluid_x = x
+    sol = _solver(params, sc)
+    sol.neighbor_search()
+    nb = sol.get_neighbors(with_boundary=True)
+    op = oracle.reference_params(diameter=0.02, w_size=1024, g_size=1024)
+    off, idx = oracle.neighbors(op, x, x, same=True)
+    assert csr_equal(nb["ff_off"], nb["ff_idx"], off, idx)
+    off, idx = oracle.neighbors(op, x, sc.boundary_x, same=False)
+    assert csr_equal(nb["fb_off"], nb["fb_idx"], off, idx)
+    sol.close()
+
+
+def test_nonfinite_input_raises():
+    from warpsph_b200._lib import SPH_E_NONFINITE, SphError
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+
+    sc = preset_scene("dam_break_8k")
+    sol = _solver(preset_params("dam_break_8k"), sc)
+    v = sc.fluid_v.copy()
+    v[123] = np.nan
+    sol.set_state(sc.fluid_x, v)
+    with pytest.raises(SphError) as e:
+        sol.step()
+    assert e.value.code == SPH_E_NONFINITE
+    sol.close()

@@ -1,0 +1,254 @@
+// Neighbour build fused with everything of the step that depends only on
+// positions and velocities.  One thread per sorted fluid particle scans the
+// 3x3 rows of 3 x-adjacent cells (9 contiguous particle ranges) of the fluid
+// grid and of the boundary grid once, and produces:
+//
+//   ELL list of fluid neighbours    count_same/store_same_neighbor (IISPH.py:52-104)
+//   fluid-boundary counts (+lists)  count_diff/store_diff_neighbor (IISPH.py:107-163)
+//   rho                             compute_density (IISPH.py:177-214)
+//   v_adv                           predict_v_adv (IISPH.py:217-278), VIS_MU = 0
+//   rho_adv                         predict_rho_adv (IISPH.py:281-329)
+//   d_ii                            compute_term_d (IISPH.py:332-382)
+//   a_ii                            compute_term_a (IISPH.py:385-428)
+//   p for the first Jacobi pass     init_pressure + update_p (IISPH.py:166-174, 521-539)
+//   B_i = sum_b psi_b gradW_ib      the boundary sum reused by every Jacobi pass
+//
+// Membership uses the reference's float32 test |x_i - x_j| < h (IISPH.py:71-72)
+// evaluated without contraction: r2 < r2_limit is exactly sqrt_rn(r2) < h.
+//
+// The per-pair vectors d_ij / d_ji the reference stores (IISPH.py:372-373,
+// 24 B per pair) are not stored: the Jacobi passes recompute gradW from
+// positions.  a_ii uses sum_j (d_ii - d_ji).gradW_ij
+//   = d_ii . sum_j gradW_ij - (m dt^2 / rho_i^2) sum_j |gradW_ij|^2,
+// both terms of which have the same sign, so the regrouping loses no accuracy.
+#include "sph_internal.cuh"
+
+namespace sph {
+
+template <bool SMEM>
+__global__ void __launch_bounds__(256) k_build(BuildArgs a) {
+  extern __shared__ float s_tab[];
+  const float* W = a.w_table;
+  const float* G = a.g_table;
+  if (SMEM) {
+    for (int t = threadIdx.x; t < a.c.sw; t += blockDim.x) s_tab[t] = a.w_table[t];
+    for (int t = threadIdx.x; t < a.c.sg; t += blockDim.x) s_tab[a.c.sw + t] = a.g_table[t];
+    __syncthreads();
+    W = s_tab;
+    G = s_tab + a.c.sw;
+  }
+  const Consts c = a.c;
+  const Grid g = a.grid;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < a.n;
+  int cnt = 0, cntb = 0;
+  if (live) {
+    const float dt = a.st->dt;
+    const float gdt = (-c.gravity) * dt;
+    const float4 xi = a.pos[i];
+    const float4 vi = a.vel[i];
+    const float vax = vi.x, vay = vi.y + gdt, vaz = vi.z;
+    const int3 ci = cell_coord(g, xi.x, xi.y, xi.z);
+    const int K = c.max_ff;
+    int* nbr = a.nbr_ff + ell_index(i, 0, K);
+
+    float sW = 0.f, sGx = 0.f, sGy = 0.f, sGz = 0.f, sG2 = 0.f, div = 0.f;
+    const int x0 = max(ci.x - 1, 0), x1 = min(ci.x + 1, g.nx - 1);
+    for (int cz = max(ci.z - 1, 0); cz <= min(ci.z + 1, g.nz - 1); ++cz) {
+      for (int cy = max(ci.y - 1, 0); cy <= min(ci.y + 1, g.ny - 1); ++cy) {
+        const int row = (cz * g.ny + cy) * g.nx;
+        const int jb = a.cell_start[row + x0], je = a.cell_start[row + x1 + 1];
+        for (int j = jb; j < je; ++j) {
+          if (j == i) continue;
+          const float4 xj = a.pos[j];
+          const float r2 = dist2_rn(xi.x, xi.y, xi.z, xj.x, xj.y, xj.z);
+          if (r2 < c.r2_limit) {
+            if (cnt < K) nbr[(long long)cnt * kWarp] = j;
+            ++cnt;
+            const float r = __fsqrt_rn(r2);
+            sW += table_lerp(W, r, c.w_scale, c.sw);
+            const float gs = grad_scalar(G, r, c);
+            const float gx = gs * (xj.x - xi.x), gy = gs * (xj.y - xi.y), gz = gs * (xj.z - xi.z);
+            sGx += gx;
+            sGy += gy;
+            sGz += gz;
+            sG2 += gx * gx + gy * gy + gz * gz;
+            const float4 vj = a.vel[j];
+            div += (vax - vj.x) * gx + (vay - (vj.y + gdt)) * gy + (vaz - vj.z) * gz;
+          }
+        }
+      }
+    }
+
+    float sWb = 0.f, Bx = 0.f, By = 0.f, Bz = 0.f, divb = 0.f;
+    if (a.nb > 0) {
+      const int KB = c.max_fb;
+      int* nbrb = a.nbr_fb ? a.nbr_fb + ell_index(i, 0, KB) : nullptr;
+      for (int cz = max(ci.z - 1, 0); cz <= min(ci.z + 1, g.nz - 1); ++cz) {
+        for (int cy = max(ci.y - 1, 0); cy <= min(ci.y + 1, g.ny - 1); ++cy) {
+          const int row = (cz * g.ny + cy) * g.nx;
+          const int jb = a.bcell_start[row + x0], je = a.bcell_start[row + x1 + 1];
+          for (int b = jb; b < je; ++b) {
+            const float4 xb = a.bpos[b];
+            const float r2 = dist2_rn(xi.x, xi.y, xi.z, xb.x, xb.y, xb.z);
+            if (r2 < c.r2_limit) {
+              if (nbrb && cntb < KB) nbrb[(long long)cntb * kWarp] = b;
+              ++cntb;
+              const float r = __fsqrt_rn(r2);
+              sWb += table_lerp(W, r, c.w_scale, c.sw) * xb.w;
+              const float gs = grad_scalar(G, r, c);
+              const float gx = gs * (xb.x - xi.x), gy = gs * (xb.y - xi.y), gz = gs * (xb.z - xi.z);
+              Bx += gx * xb.w;
+              By += gy * xb.w;
+              Bz += gz * xb.w;
+              float wx = vax, wy = vay, wz = vaz;
+              if (a.bvel) {
+                const float4 vb = a.bvel[b];
+                wx -= vb.x;
+                wy -= vb.y;
+                wz -= vb.z;
+              }
+              divb += (wx * gx + wy * gy + wz * gz) * xb.w;
+            }
+          }
+        }
+      }
+    }
+
+    // compute_density (IISPH.py:214)
+    const float rho = sW * c.m + sWb + c.w0 * c.m;
+    // predict_rho_adv (IISPH.py:329)
+    const float rho_adv = rho + (div * c.m + divb) * dt;
+    // compute_term_d (IISPH.py:382): term_1 = -sum gradW_ij, term_2 = -sum psi gradW_ib
+    const float dt2 = dt * dt;
+    const float rr = rho * rho;
+    const float dix = ((-sGx) * c.m + (-Bx)) * dt2 / rr;
+    const float diy = ((-sGy) * c.m + (-By)) * dt2 / rr;
+    const float diz = ((-sGz) * c.m + (-Bz)) * dt2 / rr;
+    // compute_term_a (IISPH.py:428)
+    const float t3 = c.m * dt2;
+    const float aii = ((dix * sGx + diy * sGy + diz * sGz) - (t3 / rr) * sG2) * c.m + (dix * Bx + diy * By + diz * Bz);
+
+    // initial pressure of the solve
+    float p;
+    if (c.warm_start == SPH_WARM_ZERO) {
+      // p_0 = 0 gives Ap_0 = 0, so the first update_p (IISPH.py:534-539) is local
+      float aa = aii;
+      if (aa > -c.inv_small && aa < c.inv_small) aa = (aa < 0.f ? -1.f : 1.f) * c.inv_small;
+      p = fmaxf(0.f + (c.rho0 - rho_adv - 0.f) * c.omega / aa, 0.f);
+    } else if (c.warm_start == SPH_WARM_HALF) {
+      p = a.pprev[i] / 2.0f;
+    } else {
+      p = fmaxf(a.pmlp[i], 0.f);
+    }
+
+    a.rho[i] = rho;
+    a.bvec[i] = make_float4(Bx, By, Bz, rho_adv);
+    a.dii_aii[i] = make_float4(dix, diy, diz, aii);
+    a.vadv[i] = make_float4(vax, vay, vaz, 0.f);
+    a.p0[i] = p;
+    a.P4[i] = make_float4(dix * p, diy * p, diz * p, p / rr);
+    a.cnt_ff[i] = cnt;
+    if (a.cnt_fb) a.cnt_fb[i] = cntb;
+
+    if (a.feat) {
+      // Warm-start MLP features (10 per particle), all O(1) after normalisation.
+      float* f = a.feat + (long long)i * 10;
+      const float inv_rho0 = 1.0f / c.rho0;
+      const float dv = div * c.m + divb;                // d(rho)/dt from advection
+      float aa = aii;
+      if (aa > -c.inv_small && aa < c.inv_small) aa = (aa < 0.f ? -1.f : 1.f) * c.inv_small;
+      const float src = (c.rho0 - rho_adv) / aa;          // unrelaxed first Jacobi guess
+      const float gmag = sqrtf(sGx * sGx + sGy * sGy + sGz * sGz) * c.m * inv_rho0 * (2.0f * c.h);
+      const float pscale = 1.0f / (c.rho0 * c.gravity * c.h * 10.0f);
+      f[0] = (rho_adv - c.rho0) * inv_rho0 * 100.0f;     // predicted density deviation (%)
+      f[1] = dv * inv_rho0 * dt * 100.0f;                 // velocity divergence, % per step
+      f[2] = aii / (t3 / rr * c.m) * 1e-2f;               // a_ii relative to its lattice scale
+      f[3] = ((c.warm_start == SPH_WARM_MLP && a.pprev) ? a.pprev[i] : 0.f) * pscale;  // previous pressure
+      f[4] = float(cnt) * (1.0f / 32.0f);                 // neighbour count
+      f[5] = sWb * inv_rho0;                              // boundary psi sum (boundary density share)
+      f[6] = gmag;                                        // |grad rho| proxy
+      f[7] = src * pscale;                                // Jacobi source term
+      f[8] = (rho - c.rho0) * inv_rho0 * 100.0f;          // current density deviation (%)
+      f[9] = float(cntb) * (1.0f / 32.0f);                // boundary neighbour count
+    }
+  }
+  // bookkeeping: overflow flags, pair totals, max counts
+  const unsigned int full = 0xffffffffu;
+  int over = live ? ((cnt > c.max_ff ? SPH_F_FF_OVERFLOW : 0) |
+                     ((a.nbr_fb && cntb > c.max_fb) ? SPH_F_FB_OVERFLOW : 0))
+                  : 0;
+  unsigned long long pf = warp_sum((unsigned long long)cnt);
+  unsigned long long pb = warp_sum((unsigned long long)cntb);
+  int mf = warp_max(cnt), mb = warp_max(cntb);
+  over = __reduce_or_sync(full, over);
+  if ((threadIdx.x & 31) == 0) {
+    if (pf) atomicAdd(&a.acc->pairs_ff, pf);
+    if (pb) atomicAdd(&a.acc->pairs_fb, pb);
+    atomicMax(&a.acc->max_ff, mf);
+    atomicMax(&a.acc->max_fb, mb);
+    if (over) atomicOr(&a.acc->flags, over);
+  }
+}
+
+// compute_boundary_density (IISPH.py:23-49): psi_b = rho0 / (W(0) + sum_{b' != b} W(r)).
+__global__ void __launch_bounds__(256) k_psi(PsiArgs a, float* psi) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.nb) return;
+  const Consts c = a.c;
+  const Grid g = a.grid;
+  const float4 xb = a.bpos[b];
+  const int3 ci = cell_coord(g, xb.x, xb.y, xb.z);
+  float rho = c.w0;
+  const int x0 = max(ci.x - 1, 0), x1 = min(ci.x + 1, g.nx - 1);
+  for (int cz = max(ci.z - 1, 0); cz <= min(ci.z + 1, g.nz - 1); ++cz)
+    for (int cy = max(ci.y - 1, 0); cy <= min(ci.y + 1, g.ny - 1); ++cy) {
+      const int row = (cz * g.ny + cy) * g.nx;
+      for (int j = a.bcell_start[row + x0]; j < a.bcell_start[row + x1 + 1]; ++j) {
+        if (j == b) continue;
+        const float4 xj = a.bpos[j];
+        const float r2 = dist2_rn(xb.x, xb.y, xb.z, xj.x, xj.y, xj.z);
+        if (r2 < c.r2_limit) rho += table_lerp(a.w_table, __fsqrt_rn(r2), c.w_scale, c.sw);
+      }
+    }
+  psi[b] = c.rho0 / rho;
+}
+
+__global__ void k_pack_psi(int nb, const float* __restrict__ psi, float4* bpos) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nb) bpos[b].w = psi[b];
+}
+
+static size_t table_bytes(const Consts& c) { return sizeof(float) * (size_t(c.sw) + size_t(c.sg)); }
+static bool tables_fit_smem(const Consts& c) { return table_bytes(c) <= 96 * 1024; }
+
+cudaError_t launch_build(const BuildArgs& a, int block, cudaStream_t s) {
+  if (a.n <= 0) return cudaSuccess;
+  const int grid = (a.n + block - 1) / block;
+  if (tables_fit_smem(a.c)) {
+    const size_t smem = table_bytes(a.c);
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k_build<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+      if (e != cudaSuccess) return e;
+    }
+    k_build<true><<<grid, block, smem, s>>>(a);
+  } else {
+    k_build<false><<<grid, block, 0, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_psi(const PsiArgs& a, int block, cudaStream_t s) {
+  if (a.nb <= 0) return cudaSuccess;
+  float* psi = nullptr;
+  cudaError_t e = cudaMallocAsync(&psi, sizeof(float) * a.nb, s);
+  if (e != cudaSuccess) return e;
+  const int grid = (a.nb + block - 1) / block;
+  k_psi<<<grid, block, 0, s>>>(a, psi);
+  k_pack_psi<<<grid, block, 0, s>>>(a.nb, psi, a.bpos);
+  e = cudaGetLastError();
+  cudaError_t f = cudaFreeAsync(psi, s);
+  return e != cudaSuccess ? e : f;
+}
+
+}  // namespace sph

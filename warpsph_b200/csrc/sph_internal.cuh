@@ -1,0 +1,279 @@
+// Internal structures and device helpers of libwpsph (sm_100a).
+//
+// Data layout (HBM), all in the cell-sorted particle order of the current step:
+//   pos  float4 (x, y, z, 0)          vel  float4 (vx, vy, vz, 0)
+//   bpos float4 (x, y, z, psi)        boundary, sorted once
+//   nbr  int32, tile-major ELL: element k of particle i sits at
+//        (i/32)*32*K + k*32 + i%32, so a warp reading its k-th neighbours
+//        issues one coalesced 128-byte load.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/wpsph.h"
+
+namespace sph {
+
+constexpr int kWarp = 32;
+
+// Uniform neighbour grid.  Cell size is slightly above h, so every neighbour
+// within h of a particle lies in the 3x3x3 cells around it even after float32
+// rounding of the cell coordinate.  Coordinates outside the grid are clamped to
+// the edge cells: clamping is monotone and 1-Lipschitz in cell space, so the
+// 27-cell search stays complete for particles that leave the domain.
+struct Grid {
+  float ox, oy, oz;  // origin
+  float inv_cell;
+  int nx, ny, nz;
+  int ncells;
+};
+
+__host__ __device__ inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+__device__ inline int3 cell_coord(const Grid& g, float x, float y, float z) {
+  int cx = __float2int_rd((x - g.ox) * g.inv_cell);
+  int cy = __float2int_rd((y - g.oy) * g.inv_cell);
+  int cz = __float2int_rd((z - g.oz) * g.inv_cell);
+  return make_int3(clampi(cx, 0, g.nx - 1), clampi(cy, 0, g.ny - 1), clampi(cz, 0, g.nz - 1));
+}
+__device__ inline int cell_index(const Grid& g, int3 c) { return (c.z * g.ny + c.y) * g.nx + c.x; }
+
+// Constants of the physics, as the float32 values the reference kernels see.
+struct Consts {
+  float h;          // fp32(SMOOTHING_LENGTH)
+  float r2_limit;   // neighbour iff r2 < r2_limit  <=>  sqrt_rn(r2) < h (exact)
+  float w_scale;    // fp32(W_SIZE-1) * fp32(1/h), as sph_funcs.py:97 evaluates it
+  float g_scale;    // fp32(GRAD_W_SIZE-1) * fp32(1/h) (sph_funcs.py:112)
+  int sw, sg;       // table sizes
+  float rho0, gravity, omega, inv_small, mu, m;
+  float w0;         // spline_W(0) = W_table[0]
+  float eta;
+  int min_iter, max_loop, fixed_iters, warm_start;
+  int max_ff, max_fb, keep_fb;
+};
+
+// Scalars carried across steps (device resident so the step needs no host sync).
+struct DevState {
+  double dt64, inv_dt64;  // dt, 1/dt with the precision the reference holds them in
+  float dt, inv_dt;       // what the kernels use (float32 kernel arguments)
+  double sim_time;
+  long long step_index;
+};
+
+// Per-step accumulators, zeroed at the start of every step.
+struct StepAcc {
+  int iterations;
+  int flags;
+  double avg_err;
+  unsigned int vmax_bits;
+  int max_ff, max_fb;
+  int pad0;
+  unsigned long long pairs_ff, pairs_fb;
+  unsigned int bar_count, bar_gen, done_blocks, pad1;
+};
+
+struct Partial {
+  double sum;
+  long long cnt;
+};
+
+constexpr int kStatsRing = 4096;
+
+// ------------------------------------------------------------------ math
+
+__device__ inline float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
+
+// Linear-interpolated table lookup of sph_funcs.py:92-102 / 105-118, for r < h.
+__device__ inline float table_lerp(const float* __restrict__ T, float r, float scale, int S) {
+  float f = r * scale;
+  int lo = min(__float2int_rz(f), S - 2);
+  float a = f - float(lo);
+  return (1.0f - a) * T[lo] + a * T[lo + 1];
+}
+
+// spline_W (sph_funcs.py:92-102)
+__device__ inline float spline_W(const float* T, float r, const Consts& c) {
+  if (r >= c.h) return 0.0f;
+  return table_lerp(T, r, c.w_scale, c.sw);
+}
+
+// Scalar part of grad_spline_W (sph_funcs.py:105-118): 0 outside (1e-10, h).
+__device__ inline float grad_scalar(const float* T, float r, const Consts& c) {
+  if (r >= c.h || r < 1e-10f) return 0.0f;
+  return table_lerp(T, r, c.g_scale, c.sg);
+}
+
+// Exact float32 |a-b|^2 as wp.length(a - b) squares it: no contraction,
+// x*x + y*y + z*z left to right.
+__device__ inline float dist2_rn(float ax, float ay, float az, float bx, float by, float bz) {
+  float dx = __fsub_rn(ax, bx), dy = __fsub_rn(ay, by), dz = __fsub_rn(az, bz);
+  return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+__device__ inline long long ell_index(long long i, int k, int K) {
+  return (i >> 5) * (long long)(kWarp * K) + (long long)k * kWarp + (i & 31);
+}
+
+// ------------------------------------------------------------------ reductions
+
+template <typename T>
+__device__ inline T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ inline int warp_max(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// ------------------------------------------------------------------ grid barrier
+
+__device__ inline unsigned int ld_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ inline int ld_volatile_int(const int* p) { return *(volatile const int*)p; }
+
+// Grid-wide barrier for a cooperative (co-resident) launch.  Every wait is
+// bounded by `budget` SM cycles; on expiry it sets SPH_F_TIMEOUT and returns
+// false, and every later barrier returns false at once, so the kernel always
+// terminates and the host reads SPH_E_TIMEOUT.
+__device__ inline bool grid_barrier(StepAcc* acc, unsigned int nblocks, long long budget) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = (ld_volatile_int(&acc->flags) & SPH_F_TIMEOUT) ? 0 : 1;
+    if (ok) {
+      unsigned int gen = ld_acquire(&acc->bar_gen);
+      __threadfence();
+      unsigned int arrived = atomicAdd(&acc->bar_count, 1u);
+      if (arrived == nblocks - 1) {
+        atomicExch(&acc->bar_count, 0u);
+        __threadfence();
+        atomicAdd(&acc->bar_gen, 1u);
+      } else {
+        long long t0 = clock64();
+        while (ld_acquire(&acc->bar_gen) == gen) {
+          if (ld_volatile_int(&acc->flags) & SPH_F_TIMEOUT) { ok = 0; break; }
+          if (clock64() - t0 > budget) {
+            atomicOr(&acc->flags, SPH_F_TIMEOUT);
+            ok = 0;
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// ------------------------------------------------------------------ kernel args
+
+struct SortArgs {
+  int n;
+  Grid grid;
+  const float4* pos;   // unsorted (current state order)
+  const int* orig;     // original id per particle of that order
+  int* key;
+  int* rank;
+  int* cell_count;     // ncells, zeroed
+  int* cell_start;     // ncells + 1
+  int* scan_part;      // partial sums per scan block
+  int* sort_src;       // new index -> old index
+  int* sort_orig;      // new index -> original id
+};
+
+struct BuildArgs {
+  int n, nb;
+  Grid grid;
+  Consts c;
+  const float* w_table;
+  const float* g_table;
+  const float4* pos;       // sorted fluid
+  const float4* vel;
+  const float* pprev;      // previous-step pressure, sorted (warm start)
+  const float* pmlp;       // MLP warm-start prediction, sorted (SPH_WARM_MLP)
+  const int* cell_start;   // fluid
+  const float4* bpos;      // sorted boundary (x, y, z, psi)
+  const float4* bvel;
+  const int* bcell_start;
+  const DevState* st;
+  StepAcc* acc;
+  int* nbr_ff;
+  int* cnt_ff;
+  int* nbr_fb;             // optional
+  int* cnt_fb;
+  float* rho;
+  float4* bvec;            // (sum_b psi_b gradW_ib, rho_adv)
+  float4* dii_aii;         // (d_ii, a_ii)
+  float4* vadv;
+  float* p0;               // initial pressure of the solve (p_1 for the zero warm start)
+  float4* P4;              // (d_ii p, p / rho^2)
+  float* feat;             // optional MLP feature rows (n x 10), NULL to skip
+};
+
+struct JacobiArgs {
+  int n;
+  Consts c;
+  const float* g_table;
+  const float4* pos;
+  const int* nbr_ff;
+  const int* cnt_ff;
+  const float* rho;
+  const float4* bvec;
+  const float4* dii_aii;
+  const float4* vadv;
+  const int* orig_w;
+  float* p_a;              // ping
+  float* p_b;              // pong
+  float4* P4;
+  float4* s4;              // (s, A1)
+  float* Ap;
+  Partial* partials;       // one per block
+  DevState* st;
+  StepAcc* acc;
+  SphStepStats* ring;      // per-step stats ring buffer
+  SphStepStats* last;      // stats of the last completed step
+  // outputs of the kick/drift epilogue (next step's state)
+  float4* pos_out;
+  float4* vel_out;
+  int* orig_out;
+  float* p_out;
+  int start_iter;          // 1: p_1 came from the build; 0: warm start, run pass 0
+  long long budget;        // barrier spin budget in SM cycles
+  double dt_max, cfl_len, inv_small_d, eta_d;
+};
+
+struct PsiArgs {
+  int nb;
+  Grid grid;
+  Consts c;
+  const float* w_table;
+  float4* bpos;            // in: x,y,z; out: w = psi
+  const int* bcell_start;
+};
+
+// launchers (host)
+cudaError_t launch_sort(const SortArgs& a, int ncells, cudaStream_t s);
+cudaError_t launch_build(const BuildArgs& a, int block, cudaStream_t s);
+cudaError_t launch_psi(const PsiArgs& a, int block, cudaStream_t s);
+cudaError_t launch_gather(int n, const int* sort_src, const int* sort_orig, const float4* pos_in,
+                          const float4* vel_in, const float* p_in, float4* pos_out, float4* vel_out,
+                          int* orig_out, float* p_out, cudaStream_t s);
+cudaError_t jacobi_config(int block, int sg, int* blocks_per_sm, size_t* smem);
+cudaError_t launch_jacobi(const JacobiArgs& a, int grid, int block, size_t smem, cudaStream_t s);
+cudaError_t launch_pack_fluid(int n, const float* x3, const float* v3, float4* pos, float4* vel, int* orig,
+                              float* p, cudaStream_t s);
+cudaError_t launch_unsort4(int n, const int* orig, const float4* src, int component, float* out, cudaStream_t s);
+cudaError_t launch_unsort1(int n, const int* orig, const float* src, float* out, cudaStream_t s);
+cudaError_t launch_sort1(int n, const int* orig, const float* src, float* out, cudaStream_t s);
+
+}  // namespace sph

@@ -1,0 +1,211 @@
+// Cell counting sort of particles (replaces wp.HashGrid.build, used at
+// IISPH.py:811 and IISPH.py:1414, and hash_grid_point_id at the 12 call sites
+// listed in IISPH.py:33-532).
+//
+// Order produced: ascending (cell index, original id).  The cell index runs x
+// fastest, so the three x-adjacent cells of a 3x3x3 neighbourhood are one
+// contiguous particle range.  Within a cell, particles are ordered by original
+// id, which makes the sorted order a pure function of the positions (no
+// dependence on atomics or on the previous step's order).
+//
+//   1. k_cell_keys   cell key per particle; rank inside its cell from a
+//                    warp-aggregated atomic on the cell counter
+//   2. k_scan_part   per-block sums of the cell counters
+//   3. k_scan_final  exclusive scan -> cell_start (each block first sums the
+//                    partials before it: no inter-block waiting)
+//   4. k_scatter     new slot = cell_start[key] + rank
+//   5. k_cell_sort   order each cell's slots by original id
+#include "sph_internal.cuh"
+
+namespace sph {
+
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 8;  // cells per thread
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__global__ void k_cell_keys(SortArgs a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool live = i < a.n;
+  int key = -1;
+  if (live) {
+    float4 x = a.pos[i];
+    key = cell_index(a.grid, cell_coord(a.grid, x.x, x.y, x.z));
+    a.key[i] = key;
+  }
+  unsigned int active = __ballot_sync(0xffffffffu, live);
+  if (!live) return;
+  // lanes sharing a cell: one atomic per group, ranks by lane order
+  unsigned int peers = __match_any_sync(active, key);
+  int leader = __ffs(peers) - 1;
+  int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(&a.cell_count[key], __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  a.rank[i] = base + __popc(peers & ((1u << lane) - 1u));
+}
+
+__device__ inline int block_sum_int(int v, int* sm) {
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  v = warp_sum(v);
+  if (lane == 0) sm[w] = v;
+  __syncthreads();
+  int nw = blockDim.x >> 5;
+  int t = (threadIdx.x < nw) ? sm[threadIdx.x] : 0;
+  if (w == 0) t = warp_sum(t);
+  __syncthreads();
+  if (threadIdx.x == 0) sm[0] = t;
+  __syncthreads();
+  int r = sm[0];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_part(const int* __restrict__ count, int ncells, int* part) {
+  __shared__ int sm[32];
+  int base = blockIdx.x * kScanTile;
+  int v = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    int c = base + k * kScanThreads + threadIdx.x;
+    if (c < ncells) v += count[c];
+  }
+  v = block_sum_int(v, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_final(const int* __restrict__ count, int ncells,
+                                                             const int* __restrict__ part, int* start, int n) {
+  __shared__ int sm[32];
+  __shared__ int warp_tot[kScanThreads / 32];
+  // prefix of earlier tiles
+  int pre = 0;
+  for (int b = threadIdx.x; b < (int)blockIdx.x; b += kScanThreads) pre += part[b];
+  pre = block_sum_int(pre, sm);
+  // each thread scans kScanItems consecutive cells
+  int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int tot = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    int c = base + k;
+    v[k] = (c < ncells) ? count[c] : 0;
+    tot += v[k];
+  }
+  // exclusive scan of thread totals
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int inc = tot;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) warp_tot[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    int t = (lane < kScanThreads / 32) ? warp_tot[lane] : 0;
+    int ti = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int u = __shfl_up_sync(0xffffffffu, ti, o);
+      if (lane >= o) ti += u;
+    }
+    if (lane < kScanThreads / 32) warp_tot[lane] = ti - t;
+  }
+  __syncthreads();
+  int run = pre + warp_tot[w] + inc - tot;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    int c = base + k;
+    if (c < ncells) start[c] = run;
+    run += v[k];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) start[ncells] = n;
+}
+
+__global__ void k_scatter(SortArgs a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  int dst = a.cell_start[a.key[i]] + a.rank[i];
+  a.sort_src[dst] = i;
+  a.sort_orig[dst] = a.orig[i];
+}
+
+// Insertion sort of one cell's slots by original id.  Cells hold ~8 particles
+// at rest density; the register path covers up to 32, larger cells sort in place.
+__global__ void k_cell_sort(const int* __restrict__ start, int ncells, int* src, int* orig) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  int b = start[c], e = start[c + 1];
+  int len = e - b;
+  if (len < 2) return;
+  if (len <= 32) {
+    int ko[32], ks[32];
+    for (int t = 0; t < len; ++t) {
+      int o = orig[b + t], s = src[b + t];
+      int u = t;
+      while (u > 0 && ko[u - 1] > o) {
+        ko[u] = ko[u - 1];
+        ks[u] = ks[u - 1];
+        --u;
+      }
+      ko[u] = o;
+      ks[u] = s;
+    }
+    for (int t = 0; t < len; ++t) {
+      orig[b + t] = ko[t];
+      src[b + t] = ks[t];
+    }
+  } else {
+    for (int t = b + 1; t < e; ++t) {
+      int o = orig[t], s = src[t];
+      int u = t;
+      while (u > b && orig[u - 1] > o) {
+        orig[u] = orig[u - 1];
+        src[u] = src[u - 1];
+        --u;
+      }
+      orig[u] = o;
+      src[u] = s;
+    }
+  }
+}
+
+__global__ void k_gather(int n, const int* __restrict__ sort_src, const int* __restrict__ sort_orig,
+                         const float4* __restrict__ pos_in, const float4* __restrict__ vel_in,
+                         const float* __restrict__ p_in, float4* __restrict__ pos_out,
+                         float4* __restrict__ vel_out, int* __restrict__ orig_out, float* __restrict__ p_out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int s = sort_src[k];
+  pos_out[k] = pos_in[s];
+  if (vel_out) vel_out[k] = vel_in[s];
+  orig_out[k] = sort_orig[k];
+  if (p_out) p_out[k] = p_in[s];
+}
+
+cudaError_t launch_sort(const SortArgs& a, int ncells, cudaStream_t s) {
+  if (a.n <= 0) return cudaMemsetAsync(a.cell_start, 0, sizeof(int) * (ncells + 1), s);
+  cudaError_t e = cudaMemsetAsync(a.cell_count, 0, sizeof(int) * ncells, s);
+  if (e != cudaSuccess) return e;
+  const int T = 256;
+  int gb = (a.n + T - 1) / T;
+  k_cell_keys<<<gb, T, 0, s>>>(a);
+  int tiles = (ncells + kScanTile - 1) / kScanTile;
+  k_scan_part<<<tiles, kScanThreads, 0, s>>>(a.cell_count, ncells, a.scan_part);
+  k_scan_final<<<tiles, kScanThreads, 0, s>>>(a.cell_count, ncells, a.scan_part, a.cell_start, a.n);
+  k_scatter<<<gb, T, 0, s>>>(a);
+  k_cell_sort<<<(ncells + T - 1) / T, T, 0, s>>>(a.cell_start, ncells, a.sort_src, a.sort_orig);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather(int n, const int* sort_src, const int* sort_orig, const float4* pos_in,
+                          const float4* vel_in, const float* p_in, float4* pos_out, float4* vel_out,
+                          int* orig_out, float* p_out, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int T = 256;
+  k_gather<<<(n + T - 1) / T, T, 0, s>>>(n, sort_src, sort_orig, pos_in, vel_in, p_in, pos_out, vel_out,
+                                        orig_out, p_out);
+  return cudaGetLastError();
+}
+
+}  // namespace sph
