@@ -33,6 +33,7 @@ extern "C" {
 #define SPH_E_NONFINITE -4 /* NaN/Inf in pressure or velocity */
 #define SPH_E_TIMEOUT -5   /* a bounded grid-wide wait expired */
 #define SPH_E_NOMEM -6     /* device allocation failed */
+#define SPH_E_TOO_LARGE -7 /* input larger than a fixed-size limit (sph_boundary_psi_noalloc) */
 
 /* SphStepStats.flags bits */
 #define SPH_F_FF_OVERFLOW 0x1
@@ -156,6 +157,31 @@ int sph_get_neighbors(SphCtx* ctx, int64_t* ff_off, int32_t* ff_idx, int64_t ff_
 int sph_get_stats(SphCtx* ctx, SphStepStats* out);
 /* Override dt / 1/dt for the next step (the reference's self.dt, self.inv_dt). */
 int sph_set_dt(SphCtx* ctx, double dt, double inv_dt);
+/* Boundary volumes psi for callers that must not allocate device memory.
+ * No counterpart in the reference: the reference always runs inside Warp,
+ * which allocates freely.  This is for callers that cannot call cudaMalloc —
+ * e.g. a host framework whose memory pool owns the device, code running while
+ * a graph is captured in a mode that rejects allocations, or real-time code
+ * that must not allocate after start-up.  The caller passes device pointers:
+ * d_xb3 (nb x 3 floats, boundary positions), d_w_table (params->w_table_size
+ * floats, the W table) and d_psi (nb floats, output in input order); it gets
+ * the same psi as sph_set_boundary computes.  The library allocates nothing:
+ * its scratch is one static device array of at most 24 MiB that every device
+ * loading the library keeps until process exit.  Limits: nb <=
+ * SPH_NOALLOC_MAX_BOUNDARY (else SPH_E_TOO_LARGE, before any GPU work) and at
+ * most SPH_NOALLOC_MAX_CELLS grid cells (a coarser grid is chosen beyond that).
+ * Runs on the calling thread's current device, on `stream` (a cudaStream_t,
+ * NULL = default stream).  The first call on each device looks up the
+ * scratch address (cudaGetSymbolAddress): make that first call before any
+ * stream capture.  The call may synchronise `stream` (it reads the table's
+ * first entry, and the grid extent when params->domain_* is empty); the psi
+ * output is complete when `stream` is next synchronised.  All calls share the
+ * scratch: calls whose GPU work overlaps (other streams or threads) race. */
+#define SPH_NOALLOC_MAX_BOUNDARY 262144
+#define SPH_NOALLOC_MAX_CELLS 1048576
+int sph_boundary_psi_noalloc(const SphParams* params, const float* d_xb3, int64_t nb, const float* d_w_table,
+                             float* d_psi, void* stream);
+
 /* ABI self-description, needs no GPU: out[0] = WPSPH_ABI_VERSION,
  * out[1] = sizeof(SphParams), out[2] = sizeof(SphStepStats). */
 int sph_abi_info(int32_t* out, int32_t count);

@@ -20,6 +20,8 @@ SPH_E_CAPACITY = -3
 SPH_E_NONFINITE = -4
 SPH_E_TIMEOUT = -5
 SPH_E_NOMEM = -6
+SPH_E_TOO_LARGE = -7
+SPH_NOALLOC_MAX_BOUNDARY = 262144
 
 SPH_F_FF_OVERFLOW = 0x1
 SPH_F_FB_OVERFLOW = 0x2
@@ -34,6 +36,7 @@ SPH_WARM_MLP = 2
 _ERRNAMES = {
     SPH_E_INVALID: "SPH_E_INVALID", SPH_E_CUDA: "SPH_E_CUDA", SPH_E_CAPACITY: "SPH_E_CAPACITY",
     SPH_E_NONFINITE: "SPH_E_NONFINITE", SPH_E_TIMEOUT: "SPH_E_TIMEOUT", SPH_E_NOMEM: "SPH_E_NOMEM",
+    SPH_E_TOO_LARGE: "SPH_E_TOO_LARGE",
 }
 
 
@@ -96,6 +99,7 @@ SIGNATURES = {
     "sph_get_stats": (ctypes.c_int, [_P, ctypes.POINTER(SphStepStats)]),
     "sph_set_dt": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double]),
     "sph_abi_info": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "sph_boundary_psi_noalloc": (ctypes.c_int, [ctypes.POINTER(SphParams), _P, ctypes.c_int64, _P, _P, _P]),
     "sph_num_fluid": (ctypes.c_int64, [_P]),
     "sph_num_boundary": (ctypes.c_int64, [_P]),
     "sph_stream": (ctypes.c_void_p, [_P]),

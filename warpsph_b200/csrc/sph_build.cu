@@ -251,4 +251,12 @@ cudaError_t launch_psi(const PsiArgs& a, int block, cudaStream_t s) {
   return e != cudaSuccess ? e : f;
 }
 
+// psi in sorted boundary order into a caller-provided buffer, with no
+// allocation (used by the no-allocation entry point).
+cudaError_t launch_psi_sorted(const PsiArgs& a, float* psi_sorted, int block, cudaStream_t s) {
+  if (a.nb <= 0) return cudaSuccess;
+  k_psi<<<(a.nb + block - 1) / block, block, 0, s>>>(a, psi_sorted);
+  return cudaGetLastError();
+}
+
 }  // namespace sph

@@ -265,6 +265,7 @@ struct PsiArgs {
 cudaError_t launch_sort(const SortArgs& a, int ncells, cudaStream_t s);
 cudaError_t launch_build(const BuildArgs& a, int block, cudaStream_t s);
 cudaError_t launch_psi(const PsiArgs& a, int block, cudaStream_t s);
+cudaError_t launch_psi_sorted(const PsiArgs& a, float* psi_sorted, int block, cudaStream_t s);
 cudaError_t launch_gather(int n, const int* sort_src, const int* sort_orig, const float4* pos_in,
                           const float4* vel_in, const float* p_in, float4* pos_out, float4* vel_out,
                           int* orig_out, float* p_out, cudaStream_t s);
