@@ -99,8 +99,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def run_cpu_reference(budget_s: float, max_steps: int, nthreads: int = 0):
-    """The reference algorithm (CPU oracle, FP32, OpenMP) on the same scene."""
+def run_cpu_reference(budget_s: float, max_steps: int, nthreads: int = 0, state=None):
+    """The reference algorithm (CPU oracle, FP32, OpenMP) on the same scene,
+    from ``state`` = (x, v, dt, step_index) when given (the GPU run's state at
+    the start of its timed region), else from the initial state."""
     from oracle import oracle
     from warpsph_b200.params import preset_params
     from warpsph_b200.scenes import preset_scene
@@ -113,8 +115,11 @@ def run_cpu_reference(budget_s: float, max_steps: int, nthreads: int = 0):
     tabs = kernel_tables(params)
     nt = nthreads or oracle.max_threads()
     psi = oracle.boundary_psi(op, scene.boundary_x, tables=tabs, nthreads=nt)
-    x, v = scene.fluid_x.copy(), scene.fluid_v.copy()
-    dt, inv_dt = params.dt_max, 1.0 / params.dt_max
+    if state is None:
+        x, v, dt, start = scene.fluid_x.copy(), scene.fluid_v.copy(), params.dt_max, 0
+    else:
+        x, v, dt, start = state
+    inv_dt = 1.0 / dt
     steps, t_total, iters = 0, 0.0, []
     while steps < max_steps and (steps == 0 or t_total < budget_s):
         t0 = time.perf_counter()
@@ -125,8 +130,8 @@ def run_cpu_reference(budget_s: float, max_steps: int, nthreads: int = 0):
         iters.append(r["iterations"])
         steps += 1
     return {"value": steps / t_total, "unit": "steps/s", "cores": nt, "kind": "port",
-            "sample": f"first {steps} steps of the 1M-particle dam break from its initial state "
-                      f"(FP32 oracle, {nt} OpenMP threads), iterations {iters}"}
+            "sample": f"steps [{start}, {start + steps}) of the 1M-particle dam break "
+                      f"(FP32 oracle, {nt} OpenMP threads); Jacobi iterations {iters}"}
 
 
 def bench_reference(args):
@@ -139,8 +144,9 @@ def bench_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 / base["value"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "dam break, 1,000,000 fluid + 206,464 boundary particles, tol 0.1% avg density err",
-                   "preset": PRESET},
+        "config": {"workload": f"dam break, 1,000,000 fluid + 206,464 boundary particles, steps [0, {args.steps}) "
+                               "from the initial state (CPU: the first steps of that range, time-bounded), "
+                               "0.1% avg density err", "preset": PRESET, "warm_start": "zero"},
         "cpu_baseline": base,
         "e2e": {"value": base["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -161,65 +167,111 @@ def bench_ours(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
     dist = None
     if world > 1:
         import datetime
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
-    params = preset_params(PRESET, device=local)
     scene = preset_scene(PRESET)
-    sol = IISPH(stage_path=None, params=params, scene=scene)
-    L, ctx = sol._lib, sol._ctx
-    stream = torch.cuda.ExternalStream(L.sph_stream(ctx), device=torch.device("cuda", local))
     n = scene.n
+    headline = args.warm
+    K = args.steps
 
-    sol.steps(args.warmup)  # also captures the step graph
+    def fresh(mode):
+        s = IISPH(stage_path=None, params=preset_params(PRESET, device=local, warm_start=mode), scene=scene)
+        _lib.check(s._ctx, s._lib.sph_prepare(s._ctx))  # capture the step graph outside any timing
+        return s
+
+    def stream_of(s):
+        return torch.cuda.ExternalStream(s._lib.sph_stream(s._ctx), device=dev)
+
+    def check_flags(hist):
+        flags = 0
+        for h in hist:
+            flags |= h["flags"]
+        bad = _lib.SPH_F_TIMEOUT | _lib.SPH_F_NONFINITE | _lib.SPH_F_FF_OVERFLOW | _lib.SPH_F_FB_OVERFLOW
+        if flags & bad:
+            raise RuntimeError(f"step flags {flags:#x} in a timed region")
+
+    def timed_steps(s, count):
+        st = stream_of(s)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        _lib.check(s._ctx, s._lib.sph_launch_steps(s._ctx, count))
+        e1.record(st)
+        e1.synchronize()
+        hist = s.stats_history(count)
+        check_flags(hist)
+        return e0.elapsed_time(e1), hist
+
+    # warm-up: W steps on a throwaway solver (clocks, module load, graph capture)
+    w = fresh(headline)
+    if args.warmup:
+        w.steps(args.warmup)
+    w.close()
+
+    if args.profile:
+        # minimal launch sequence for ncu: K steps from the initial state
+        s = fresh(headline)
+        _lib.check(s._ctx, s._lib.sph_launch_steps(s._ctx, K))
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_run": True, "steps": K, "stats": s.stats_history(K)[-1]}))
+        s.close()
+        return
+
+    # timed region: steps [0, K) of the dam break from its initial state
+    sol = fresh(headline)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    _lib.check(ctx, L.sph_launch_steps(ctx, args.steps))
-    ev1.record(stream)
-    ev1.synchronize()
+    ms, hist = timed_steps(sol, K)
     clock = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    hist = sol.stats_history(args.steps)
-    flags = 0
-    for h in hist:
-        flags |= h["flags"]
-    if flags & (_lib.SPH_F_TIMEOUT | _lib.SPH_F_NONFINITE | _lib.SPH_F_FF_OVERFLOW | _lib.SPH_F_FB_OVERFLOW):
-        raise RuntimeError(f"step flags {flags:#x} in the timed region")
-    iters = [h["iterations"] for h in hist]
-    errs = [h["avg_err"] for h in hist]
-    pairs = [h["n_ff_pairs"] for h in hist]
-    ms_t = torch.tensor([ms], device="cuda")
+    sol.close()
+    ms_t = torch.tensor([ms], device=dev)
     if dist:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
     ms_max = float(ms_t.item())
-    value = world * args.steps / (ms_max / 1000.0)
+    value = world * K / (ms_max / 1000.0)
+    iters = [h["iterations"] for h in hist]
 
-    # dominant kernel (the persistent Jacobi solve): per-launch CUDA-event time
-    kt = min(args.steps, 20)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(kt)]
-    evf = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(kt)]
-    for a, b in zip(evs, evf):
-        b[0].record(stream)
-        _lib.check(ctx, L.sph_launch_phase(ctx, 0))
-        b[1].record(stream)
-        a[0].record(stream)
-        _lib.check(ctx, L.sph_launch_phase(ctx, 1))
-        a[1].record(stream)
+    # the same K steps with the other warm-start modes (context for the headline)
+    modes = {}
+    for mode in ("zero", "half"):
+        if mode == headline:
+            modes[mode] = {"steps_per_s": K / (ms / 1000.0), "jacobi_iterations": int(sum(iters))}
+            continue
+        s = fresh(mode)
+        m_ms, m_hist = timed_steps(s, K)
+        s.close()
+        modes[mode] = {"steps_per_s": K / (m_ms / 1000.0),
+                       "jacobi_iterations": int(sum(h["iterations"] for h in m_hist))}
+
+    # dominant kernel: per-launch CUDA-event time of the persistent solve over the same K steps
+    s = fresh(headline)
+    st = stream_of(s)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(K)]
     torch.cuda.synchronize()
-    hk = sol.stats_history(kt)
-    t_jac = [a.elapsed_time(b) for a, b in evs]
-    t_front = [a.elapsed_time(b) for a, b in evf]
+    for e in ev:
+        e[0].record(st)
+        _lib.check(s._ctx, s._lib.sph_launch_phase(s._ctx, 0))
+        e[1].record(st)
+        e[2].record(st)
+        _lib.check(s._ctx, s._lib.sph_launch_phase(s._ctx, 1))
+        e[3].record(st)
+    torch.cuda.synchronize()
+    hk = s.stats_history(K)
+    check_flags(hk)
+    s.close()
+    t_front = [e[0].elapsed_time(e[1]) for e in ev]
+    t_jac = [e[2].elapsed_time(e[3]) for e in ev]
     bytes_launch = [h["iterations"] * (100.0 * n + 8.0 * h["n_ff_pairs"]) + 112.0 * n for h in hk]
     achieved = sum(bytes_launch) / (sum(t_jac) / 1000.0) / 1e9
     peak, peak_kind = _peaks()
@@ -230,52 +282,58 @@ def bench_ours(args):
 
     # end to end through the C ABI with host buffers: every step uploads its
     # input state (x, v) from pinned memory and reads back x, v, p
-    e2e_steps = min(args.steps, 10)
+    s = fresh(headline)
+    L, ctx = s._lib, s._ctx
     hx = torch.from_numpy(scene.fluid_x.copy()).pin_memory()
     hv = torch.from_numpy(scene.fluid_v.copy()).pin_memory()
     hp = torch.zeros(n, dtype=torch.float32).pin_memory()
-    sol.set_dt(params.dt_max)
-    st = _lib.SphStepStats()
+    stt = _lib.SphStepStats()
     vp = ctypes.c_void_p
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+    for _ in range(K):
         _lib.check(ctx, L.sph_set_fluid(ctx, vp(hx.data_ptr()), vp(hv.data_ptr()), n))
-        _lib.check(ctx, L.sph_step(ctx, ctypes.byref(st)))
+        if headline != "zero":
+            _lib.check(ctx, L.sph_set_pressure(ctx, vp(hp.data_ptr()), n))
+        _lib.check(ctx, L.sph_step(ctx, ctypes.byref(stt)))
         _lib.check(ctx, L.sph_get_fluid(ctx, vp(hx.data_ptr()), vp(hv.data_ptr()), vp(hp.data_ptr()), None, None))
     e2e_s = time.perf_counter() - t0
-    e2e_t = torch.tensor([e2e_s], device="cuda")
+    s.close()
+    e2e_t = torch.tensor([e2e_s], device=dev)
     if dist:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world * e2e_steps / float(e2e_t.item())
+    e2e_value = world * K / float(e2e_t.item())
+    h2d = 24 * n + (4 * n if headline != "zero" else 0)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = run_cpu_reference(budget_s=20.0, max_steps=3)
+        cpu = run_cpu_reference(budget_s=20.0, max_steps=K)
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": ms_max / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "dam break, 1,000,000 fluid + 206,464 boundary particles, tol 0.1% avg density err",
-                       "preset": PRESET, "warm_start": params.warm_start, "parallelism": f"replicas{world}",
+            "config": {"workload": f"dam break, 1,000,000 fluid + 206,464 boundary particles, steps [0, {K}) "
+                                   "from the initial state, 0.1% avg density err",
+                       "preset": PRESET, "warm_start": headline, "parallelism": f"replicas{world}",
                        "l2": "working set > 126 MB L2 (no flush needed)"},
+            "warm_start_modes": modes,
             "particle_updates_per_s": value * n,
-            "jacobi_iterations_mean": float(np.mean(iters)), "avg_err_max": float(np.max(errs)),
-            "n_ff_pairs_mean": float(np.mean(pairs)),
-            "phase_ms": {"front": float(np.mean(t_front)), "solve": float(np.mean(t_jac))},
+            "jacobi_iterations_mean": float(np.mean(iters)), "avg_err_max": float(np.max([h["avg_err"] for h in hist])),
+            "n_ff_pairs_mean": float(np.mean([h["n_ff_pairs"] for h in hist])),
+            "phase_ms_mean": {"front": float(np.mean(t_front)), "solve": float(np.mean(t_jac))},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_jacobi (persistent solve + kick/drift)"},
+                         "kernel": "k_jacobi (persistent solve + kick/drift)",
+                         "bytes_rule": "per launch: iterations * (100 N + 8 P_ff) + 112 N"},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 24 * n,
+            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": 28 * n + 80},
-            "gpu_launches": KERNELS_PER_STEP * args.steps,
+            "gpu_launches": KERNELS_PER_STEP * K,
             "clocks": clock,
         }
         print(json.dumps(line), flush=True)
-    sol.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -284,10 +342,13 @@ def bench_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=500)  # the 1M dam break's 500-step run
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="only warm-up + K steps (for ncu captures)")
+    ap.add_argument("--warm", choices=["zero", "half", "mlp"], default="zero",
+                    help="warm start of the headline run (zero = the reference's p <- 0)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -70,7 +70,7 @@ typedef struct SphParams {
   int32_t warm_start;    /* SPH_WARM_* */
   int32_t max_ff;        /* fluid-fluid neighbour capacity per particle */
   int32_t max_fb;        /* fluid-boundary neighbour capacity per particle */
-  int32_t keep_fb_lists; /* also store fluid-boundary lists (for sph_get_neighbors) */
+  int32_t keep_fb_lists; /* unused (fluid-boundary lists are always kept); must be 0 or 1 */
   int32_t use_graph;     /* replay the step as a CUDA graph */
   int32_t device;        /* CUDA device ordinal */
   int32_t block_size;    /* threads per block for particle kernels (0 = auto) */
@@ -134,6 +134,9 @@ int sph_get_stats_history(SphCtx* ctx, SphStepStats* out, int32_t count);
  * build + advection prediction, 1 = pressure solve + kick/drift/CFL), with no
  * host synchronisation.  Flags surface at the next sph_get_stats/sph_step. */
 int sph_launch_steps(SphCtx* ctx, int32_t nsteps);
+/* Capture the step's CUDA graph now (it is otherwise captured by the first
+ * step), so that a caller's first timed step excludes the capture. */
+int sph_prepare(SphCtx* ctx);
 int sph_launch_phase(SphCtx* ctx, int32_t phase);
 
 /* IISPH.neighbor_search() (IISPH.py:1408-1482): cell sort + neighbour build +
@@ -149,8 +152,7 @@ int sph_get_terms(SphCtx* ctx, float* d_ii3, float* a_ii, float* s3, float* v_ad
 /* boundary_x and boundary_phi (IISPH.py:789, 990) in original boundary order. */
 int sph_get_boundary(SphCtx* ctx, float* xb3, float* psi);
 /* Neighbour sets of the last build in original ids, CSR per fluid particle,
- * ids ascending (ff_neighbor_* / fs_neighbor_*, IISPH.py:798-805).
- * fb lists need params.keep_fb_lists. */
+ * ids ascending (ff_neighbor_* / fs_neighbor_*, IISPH.py:798-805). */
 int sph_get_neighbors(SphCtx* ctx, int64_t* ff_off, int32_t* ff_idx, int64_t ff_cap,
                       int64_t* fb_off, int32_t* fb_idx, int64_t fb_cap);
 

@@ -25,18 +25,64 @@
 
 namespace sph {
 
+// Phase 1 of the build for one particle: filter the candidates of the 3x3
+// rows of 3 x-adjacent cells with the exact float32 test and write the hits
+// into the particle's ELL list.  Only a compare and a predicated store run per
+// candidate, so the warp stays converged; loads are issued four at a time.
+__device__ inline int filter_rows(const Grid& g, int3 ci, const int* __restrict__ cell_start,
+                                  const float4* __restrict__ pts, float4 xi, float r2_limit, int self, int* out,
+                                  int K) {
+  int cnt = 0;
+  const int x0 = max(ci.x - 1, 0), x1 = min(ci.x + 1, g.nx - 1);
+  for (int cz = max(ci.z - 1, 0); cz <= min(ci.z + 1, g.nz - 1); ++cz) {
+    for (int cy = max(ci.y - 1, 0); cy <= min(ci.y + 1, g.ny - 1); ++cy) {
+      const int row = (cz * g.ny + cy) * g.nx;
+      const int jb = __ldg(cell_start + row + x0), je = __ldg(cell_start + row + x1 + 1);
+      int j = jb;
+      for (; j + 4 <= je; j += 4) {
+        float4 q[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) q[u] = __ldg(pts + j + u);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const float r2 = dist2_rn(xi.x, xi.y, xi.z, q[u].x, q[u].y, q[u].z);
+          if (r2 < r2_limit && j + u != self) {
+            if (cnt < K) out[(long long)cnt * kWarp] = j + u;
+            ++cnt;
+          }
+        }
+      }
+      for (; j < je; ++j) {
+        const float4 q = __ldg(pts + j);
+        const float r2 = dist2_rn(xi.x, xi.y, xi.z, q.x, q.y, q.z);
+        if (r2 < r2_limit && j != self) {
+          if (cnt < K) out[(long long)cnt * kWarp] = j;
+          ++cnt;
+        }
+      }
+    }
+  }
+  return cnt;
+}
+
+template <class Tab>
+__device__ __forceinline__ void build_body(const BuildArgs& a, const Tab& W, const Tab& G);
+
 template <bool SMEM>
 __global__ void __launch_bounds__(256) k_build(BuildArgs a) {
-  extern __shared__ float s_tab[];
-  const float* W = a.w_table;
-  const float* G = a.g_table;
+  extern __shared__ float2 s_pairs[];
   if (SMEM) {
-    for (int t = threadIdx.x; t < a.c.sw; t += blockDim.x) s_tab[t] = a.w_table[t];
-    for (int t = threadIdx.x; t < a.c.sg; t += blockDim.x) s_tab[a.c.sw + t] = a.g_table[t];
+    stage_pairs(s_pairs, a.w_table, a.c.sw);
+    stage_pairs(s_pairs + a.c.sw, a.g_table, a.c.sg);
     __syncthreads();
-    W = s_tab;
-    G = s_tab + a.c.sw;
+    build_body(a, PairTable{s_pairs}, PairTable{s_pairs + a.c.sw});
+  } else {
+    build_body(a, FlatTable{a.w_table}, FlatTable{a.g_table});
   }
+}
+
+template <class Tab>
+__device__ __forceinline__ void build_body(const BuildArgs& a, const Tab& W, const Tab& G) {
   const Consts c = a.c;
   const Grid g = a.grid;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -49,70 +95,67 @@ __global__ void __launch_bounds__(256) k_build(BuildArgs a) {
     const float4 vi = a.vel[i];
     const float vax = vi.x, vay = vi.y + gdt, vaz = vi.z;
     const int3 ci = cell_coord(g, xi.x, xi.y, xi.z);
-    const int K = c.max_ff;
+    const int K = c.max_ff, KB = c.max_fb;
     int* nbr = a.nbr_ff + ell_index(i, 0, K);
+    int* nbrb = a.nbr_fb + ell_index(i, 0, KB);
 
+    // phase 1: neighbour lists
+    cnt = filter_rows(g, ci, a.cell_start, a.pos, xi, c.r2_limit, i, nbr, K);
+    if (a.nb > 0) cntb = filter_rows(g, ci, a.bcell_start, a.bpos, xi, c.r2_limit, -1, nbrb, KB);
+
+    // phase 2: everything summed over the neighbours, in list (= ascending j) order
     float sW = 0.f, sGx = 0.f, sGy = 0.f, sGz = 0.f, sG2 = 0.f, div = 0.f;
-    const int x0 = max(ci.x - 1, 0), x1 = min(ci.x + 1, g.nx - 1);
-    for (int cz = max(ci.z - 1, 0); cz <= min(ci.z + 1, g.nz - 1); ++cz) {
-      for (int cy = max(ci.y - 1, 0); cy <= min(ci.y + 1, g.ny - 1); ++cy) {
-        const int row = (cz * g.ny + cy) * g.nx;
-        const int jb = a.cell_start[row + x0], je = a.cell_start[row + x1 + 1];
-        for (int j = jb; j < je; ++j) {
-          if (j == i) continue;
-          const float4 xj = a.pos[j];
-          const float r2 = dist2_rn(xi.x, xi.y, xi.z, xj.x, xj.y, xj.z);
-          if (r2 < c.r2_limit) {
-            if (cnt < K) nbr[(long long)cnt * kWarp] = j;
-            ++cnt;
-            const float r = __fsqrt_rn(r2);
-            sW += table_lerp(W, r, c.w_scale, c.sw);
-            const float gs = grad_scalar(G, r, c);
-            const float gx = gs * (xj.x - xi.x), gy = gs * (xj.y - xi.y), gz = gs * (xj.z - xi.z);
-            sGx += gx;
-            sGy += gy;
-            sGz += gz;
-            sG2 += gx * gx + gy * gy + gz * gz;
-            const float4 vj = a.vel[j];
-            div += (vax - vj.x) * gx + (vay - (vj.y + gdt)) * gy + (vaz - vj.z) * gz;
-          }
-        }
+    auto fluid = [&](float4 xj, float4 vj) {
+      const float r = __fsqrt_rn(dist2_rn(xi.x, xi.y, xi.z, xj.x, xj.y, xj.z));
+      sW += table_lerp(W, r, c.w_scale, c.sw);
+      const float gs = grad_scalar(G, r, c);
+      const float gx = gs * (xj.x - xi.x), gy = gs * (xj.y - xi.y), gz = gs * (xj.z - xi.z);
+      sGx += gx;
+      sGy += gy;
+      sGz += gz;
+      sG2 += gx * gx + gy * gy + gz * gz;
+      div += (vax - vj.x) * gx + (vay - (vj.y + gdt)) * gy + (vaz - vj.z) * gz;
+    };
+    const int nf = min(cnt, K);
+    int k = 0;
+    for (; k + 4 <= nf; k += 4) {
+      int j[4];
+      float4 xj[4], vj[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) j[u] = nbr[(k + u) * kWarp];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        xj[u] = __ldg(a.pos + j[u]);
+        vj[u] = __ldg(a.vel + j[u]);
       }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) fluid(xj[u], vj[u]);
+    }
+    for (; k < nf; ++k) {
+      const int j = nbr[k * kWarp];
+      fluid(__ldg(a.pos + j), __ldg(a.vel + j));
     }
 
     float sWb = 0.f, Bx = 0.f, By = 0.f, Bz = 0.f, divb = 0.f;
-    if (a.nb > 0) {
-      const int KB = c.max_fb;
-      int* nbrb = a.nbr_fb ? a.nbr_fb + ell_index(i, 0, KB) : nullptr;
-      for (int cz = max(ci.z - 1, 0); cz <= min(ci.z + 1, g.nz - 1); ++cz) {
-        for (int cy = max(ci.y - 1, 0); cy <= min(ci.y + 1, g.ny - 1); ++cy) {
-          const int row = (cz * g.ny + cy) * g.nx;
-          const int jb = a.bcell_start[row + x0], je = a.bcell_start[row + x1 + 1];
-          for (int b = jb; b < je; ++b) {
-            const float4 xb = a.bpos[b];
-            const float r2 = dist2_rn(xi.x, xi.y, xi.z, xb.x, xb.y, xb.z);
-            if (r2 < c.r2_limit) {
-              if (nbrb && cntb < KB) nbrb[(long long)cntb * kWarp] = b;
-              ++cntb;
-              const float r = __fsqrt_rn(r2);
-              sWb += table_lerp(W, r, c.w_scale, c.sw) * xb.w;
-              const float gs = grad_scalar(G, r, c);
-              const float gx = gs * (xb.x - xi.x), gy = gs * (xb.y - xi.y), gz = gs * (xb.z - xi.z);
-              Bx += gx * xb.w;
-              By += gy * xb.w;
-              Bz += gz * xb.w;
-              float wx = vax, wy = vay, wz = vaz;
-              if (a.bvel) {
-                const float4 vb = a.bvel[b];
-                wx -= vb.x;
-                wy -= vb.y;
-                wz -= vb.z;
-              }
-              divb += (wx * gx + wy * gy + wz * gz) * xb.w;
-            }
-          }
-        }
+    const int nbh = min(cntb, KB);
+    for (int t = 0; t < nbh; ++t) {
+      const int b = nbrb[t * kWarp];
+      const float4 xb = __ldg(a.bpos + b);
+      const float r = __fsqrt_rn(dist2_rn(xi.x, xi.y, xi.z, xb.x, xb.y, xb.z));
+      sWb += table_lerp(W, r, c.w_scale, c.sw) * xb.w;
+      const float gs = grad_scalar(G, r, c);
+      const float gx = gs * (xb.x - xi.x), gy = gs * (xb.y - xi.y), gz = gs * (xb.z - xi.z);
+      Bx += gx * xb.w;
+      By += gy * xb.w;
+      Bz += gz * xb.w;
+      float wx = vax, wy = vay, wz = vaz;
+      if (a.bvel) {
+        const float4 vb = __ldg(a.bvel + b);
+        wx -= vb.x;
+        wy -= vb.y;
+        wz -= vb.z;
       }
+      divb += (wx * gx + wy * gy + wz * gz) * xb.w;
     }
 
     // compute_density (IISPH.py:214)
@@ -175,9 +218,7 @@ __global__ void __launch_bounds__(256) k_build(BuildArgs a) {
   }
   // bookkeeping: overflow flags, pair totals, max counts
   const unsigned int full = 0xffffffffu;
-  int over = live ? ((cnt > c.max_ff ? SPH_F_FF_OVERFLOW : 0) |
-                     ((a.nbr_fb && cntb > c.max_fb) ? SPH_F_FB_OVERFLOW : 0))
-                  : 0;
+  int over = live ? ((cnt > c.max_ff ? SPH_F_FF_OVERFLOW : 0) | (cntb > c.max_fb ? SPH_F_FB_OVERFLOW : 0)) : 0;
   unsigned long long pf = warp_sum((unsigned long long)cnt);
   unsigned long long pb = warp_sum((unsigned long long)cntb);
   int mf = warp_max(cnt), mb = warp_max(cntb);
@@ -219,7 +260,7 @@ __global__ void k_pack_psi(int nb, const float* __restrict__ psi, float4* bpos) 
   if (b < nb) bpos[b].w = psi[b];
 }
 
-static size_t table_bytes(const Consts& c) { return sizeof(float) * (size_t(c.sw) + size_t(c.sg)); }
+static size_t table_bytes(const Consts& c) { return sizeof(float2) * (size_t(c.sw) + size_t(c.sg)); }
 static bool tables_fit_smem(const Consts& c) { return table_bytes(c) <= 96 * 1024; }
 
 cudaError_t launch_build(const BuildArgs& a, int block, cudaStream_t s) {

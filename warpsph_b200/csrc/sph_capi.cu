@@ -305,8 +305,7 @@ int sort_boundary(SphCtx* ctx) {
 int alloc_neighbors(SphCtx* ctx) {
   const int64_t tiles = (ctx->n_cap + 31) / 32;
   CK(dalloc(ctx->nbr_ff, tiles * 32 * int64_t(ctx->K_ff)));
-  if (ctx->P.keep_fb_lists) CK(dalloc(ctx->nbr_fb, tiles * 32 * int64_t(ctx->K_fb)));
-  else dfree(ctx->nbr_fb);
+  CK(dalloc(ctx->nbr_fb, tiles * 32 * int64_t(ctx->K_fb)));
   make_consts(ctx);
   ctx->graph_dirty = true;
   return SPH_OK;
@@ -389,7 +388,7 @@ sph::BuildArgs build_args(SphCtx* ctx) {
   b.acc = ctx->acc;
   b.nbr_ff = ctx->nbr_ff;
   b.cnt_ff = ctx->cnt_ff;
-  b.nbr_fb = ctx->P.keep_fb_lists ? ctx->nbr_fb : nullptr;
+  b.nbr_fb = ctx->nbr_fb;
   b.cnt_fb = ctx->cnt_fb;
   b.rho = ctx->rho;
   b.bvec = ctx->bvec;
@@ -469,32 +468,37 @@ int ensure_ready(SphCtx* ctx) {
   return SPH_OK;
 }
 
+// Capture the step into a CUDA graph (once per configuration).  Falls back to
+// plain launches of the same kernels if this runtime cannot capture them.
+int ensure_graph(SphCtx* ctx) {
+  if (!ctx->P.use_graph || !ctx->graph_ok) return SPH_OK;
+  if (!ctx->graph_dirty && ctx->gexec) return SPH_OK;
+  if (ctx->gexec) {
+    cudaGraphExecDestroy(ctx->gexec);
+    ctx->gexec = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  int erc = enqueue_step(ctx);
+  cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+  if (erc == SPH_OK && ce == cudaSuccess) ce = cudaGraphInstantiate(&ctx->gexec, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (erc != SPH_OK || ce != cudaSuccess) {
+    cudaGetLastError();
+    ctx->graph_ok = false;
+    ctx->gexec = nullptr;
+    return SPH_OK;
+  }
+  ctx->graph_dirty = false;
+  return SPH_OK;
+}
+
 int launch_step(SphCtx* ctx) {
   int rc = ensure_ready(ctx);
   if (rc) return rc;
-  if (ctx->P.use_graph && ctx->graph_ok) {
-    if (ctx->graph_dirty || !ctx->gexec) {
-      if (ctx->gexec) {
-        cudaGraphExecDestroy(ctx->gexec);
-        ctx->gexec = nullptr;
-      }
-      cudaGraph_t g = nullptr;
-      CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-      int erc = enqueue_step(ctx);
-      cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
-      if (erc == SPH_OK && ce == cudaSuccess) {
-        ce = cudaGraphInstantiate(&ctx->gexec, g, 0);
-      }
-      if (g) cudaGraphDestroy(g);
-      if (erc != SPH_OK || ce != cudaSuccess) {
-        // capture unsupported here: run the same kernels without a graph
-        cudaGetLastError();
-        ctx->graph_ok = false;
-        ctx->gexec = nullptr;
-        return enqueue_step(ctx);
-      }
-      ctx->graph_dirty = false;
-    }
+  rc = ensure_graph(ctx);
+  if (rc) return rc;
+  if (ctx->gexec) {
     CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
     return SPH_OK;
   }
@@ -516,7 +520,7 @@ int grow_capacity(SphCtx* ctx, int max_ff, int max_fb) {
     ctx->K_ff = ((max_ff + max_ff / 4 + 7) / 8) * 8;
     grow = true;
   }
-  if (ctx->P.keep_fb_lists && max_fb > ctx->K_fb) {
+  if (max_fb > ctx->K_fb) {
     ctx->K_fb = ((max_fb + max_fb / 4 + 7) / 8) * 8;
     grow = true;
   }
@@ -790,6 +794,17 @@ int sph_launch_steps(SphCtx* ctx, int32_t nsteps) {
   return SPH_OK;
 }
 
+int sph_prepare(SphCtx* ctx) {
+  if (!ctx) return SPH_E_INVALID;
+  CK(cudaSetDevice(ctx->dev));
+  int rc = ensure_ready(ctx);
+  if (rc) return rc;
+  rc = ensure_graph(ctx);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SPH_OK;
+}
+
 int sph_launch_phase(SphCtx* ctx, int32_t phase) {
   if (!ctx || phase < 0 || phase > 1) return fail(ctx, SPH_E_INVALID, "phase must be 0 or 1");
   CK(cudaSetDevice(ctx->dev));
@@ -958,7 +973,6 @@ int sph_get_neighbors(SphCtx* ctx, int64_t* ff_off, int32_t* ff_idx, int64_t ff_
     if (rc) return rc;
   }
   if (fb_off) {
-    if (!ctx->P.keep_fb_lists) return fail(ctx, SPH_E_INVALID, "fluid-boundary lists need keep_fb_lists");
     std::vector<int> bo(std::max<int64_t>(ctx->nb, 1));
     if (ctx->nb) CK(cudaMemcpy(bo.data(), ctx->borig, sizeof(int) * ctx->nb, cudaMemcpyDeviceToHost));
     int rc = export_lists(ctx->nbr_fb, ctx->cnt_fb, ctx->K_fb, bo.data(), fb_off, fb_idx, fb_cap);

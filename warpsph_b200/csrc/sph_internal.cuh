@@ -84,24 +84,49 @@ constexpr int kStatsRing = 4096;
 
 __device__ inline float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
 
-// Linear-interpolated table lookup of sph_funcs.py:92-102 / 105-118, for r < h.
-__device__ inline float table_lerp(const float* __restrict__ T, float r, float scale, int S) {
-  float f = r * scale;
-  int lo = min(__float2int_rz(f), S - 2);
-  float a = f - float(lo);
-  return (1.0f - a) * T[lo] + a * T[lo + 1];
+// Kernel tables.  A lookup needs the two samples bracketing r; the shared-memory
+// copy stores them as float2 pairs (T[k], T[k+1]) so one 8-byte load serves a
+// lookup (half the shared-memory wavefronts of two 4-byte loads).  Large tables
+// (the reference's 65536-sample gradient table) stay in global memory.
+struct FlatTable {
+  const float* T;
+  __device__ __forceinline__ float2 pair(int lo) const { return make_float2(__ldg(T + lo), __ldg(T + lo + 1)); }
+};
+struct PairTable {
+  const float2* P;
+  __device__ __forceinline__ float2 pair(int lo) const { return P[lo]; }
+};
+
+// Linear interpolation of sph_funcs.py:97-102 / 112-117, for r < h.
+template <class Tab>
+__device__ __forceinline__ float table_lerp(const Tab& t, float r, float scale, int S) {
+  const float f = r * scale;
+  const int lo = min(__float2int_rz(f), S - 2);
+  const float a = f - float(lo);
+  const float2 p = t.pair(lo);
+  return (1.0f - a) * p.x + a * p.y;
+}
+__device__ __forceinline__ float table_lerp(const float* T, float r, float scale, int S) {
+  return table_lerp(FlatTable{T}, r, scale, S);
 }
 
 // spline_W (sph_funcs.py:92-102)
-__device__ inline float spline_W(const float* T, float r, const Consts& c) {
+template <class Tab>
+__device__ __forceinline__ float spline_W(const Tab& T, float r, const Consts& c) {
   if (r >= c.h) return 0.0f;
   return table_lerp(T, r, c.w_scale, c.sw);
 }
 
 // Scalar part of grad_spline_W (sph_funcs.py:105-118): 0 outside (1e-10, h).
-__device__ inline float grad_scalar(const float* T, float r, const Consts& c) {
+template <class Tab>
+__device__ __forceinline__ float grad_scalar(const Tab& T, float r, const Consts& c) {
   if (r >= c.h || r < 1e-10f) return 0.0f;
   return table_lerp(T, r, c.g_scale, c.sg);
+}
+
+// Stage a table into shared memory as (T[k], T[k+1]) pairs, k < S-1.
+__device__ __forceinline__ void stage_pairs(float2* dst, const float* __restrict__ T, int S) {
+  for (int k = threadIdx.x; k < S - 1; k += blockDim.x) dst[k] = make_float2(T[k], T[k + 1]);
 }
 
 // Exact float32 |a-b|^2 as wp.length(a - b) squares it: no contraction,

@@ -27,18 +27,59 @@ namespace sph {
 
 constexpr int kJacobiThreads = 256;
 
-__device__ inline void pass_a(int i, const JacobiArgs& a, const float* G, float t3) {
+// Neighbour loops are unrolled by kUnroll with every load of a group issued
+// before any use, and the next group's indices are fetched while the current
+// group's gathers are in flight, so each thread keeps up to 2*kUnroll
+// independent loads outstanding (the passes are bound by gather latency).
+// List entries are read once per pass with the streaming hint (ld.global.cs),
+// which lets the L2 keep the gathered pos / P4 / s4 arrays resident instead of
+// the list stream.  Positions and counts are read-only for the whole kernel and
+// use the non-coherent path; P4 and s4 are rewritten between barriers and use
+// plain coherent loads.
+constexpr int kUnroll = 4;
+
+template <typename Body>
+__device__ __forceinline__ void for_neighbours(const int* nb, int cnt, const float4* pos, const float4* other,
+                                               Body body) {
+  int k = 0;
+  int jn[kUnroll];
+  if (cnt >= kUnroll) {
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) jn[u] = __ldcs(nb + u * kWarp);
+  }
+  for (; k + kUnroll <= cnt; k += kUnroll) {
+    int j[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) j[u] = jn[u];
+    if (k + 2 * kUnroll <= cnt) {
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) jn[u] = __ldcs(nb + (k + kUnroll + u) * kWarp);
+    }
+    float4 xj[kUnroll], oj[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      xj[u] = __ldg(pos + j[u]);
+      oj[u] = other[j[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) body(xj[u], oj[u]);
+  }
+  for (; k < cnt; ++k) {
+    const int j = __ldcs(nb + k * kWarp);
+    body(__ldg(pos + j), other[j]);
+  }
+}
+
+template <class Tab>
+__device__ inline void pass_a(int i, const JacobiArgs& a, const Tab& G, float t3) {
   const Consts& c = a.c;
-  const float4 xi = a.pos[i];
+  const float4 xi = __ldg(a.pos + i);
   const float4 qi = a.P4[i];
   const float ci = t3 * qi.w;  // d_ji p_i = gradW_ij * (m dt^2 p_i / rho_i^2)
-  const int cnt = min(a.cnt_ff[i], c.max_ff);
+  const int cnt = min(__ldg(a.cnt_ff + i), c.max_ff);
   const int* nb = a.nbr_ff + ell_index(i, 0, c.max_ff);
   float sx = 0.f, sy = 0.f, sz = 0.f, a1 = 0.f;
-  for (int k = 0; k < cnt; ++k) {
-    const int j = nb[k * kWarp];
-    const float4 xj = a.pos[j];
-    const float4 qj = a.P4[j];
+  for_neighbours(nb, cnt, a.pos, a.P4, [&](const float4 xj, const float4 qj) {
     const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
     const float r = sqrtf(dx * dx + dy * dy + dz * dz);
     const float gs = grad_scalar(G, r, c);
@@ -47,29 +88,27 @@ __device__ inline void pass_a(int i, const JacobiArgs& a, const float* G, float 
     sy += gy * qj.w;
     sz += gz * qj.w;
     a1 += (ci * gx - qj.x) * gx + (ci * gy - qj.y) * gy + (ci * gz - qj.z) * gz;
-  }
+  });
   a.s4[i] = make_float4(-t3 * sx, -t3 * sy, -t3 * sz, a1 * c.m);
 }
 
-__device__ inline void pass_b(int i, const JacobiArgs& a, const float* G, const float* pc, float* pn,
+template <class Tab>
+__device__ inline void pass_b(int i, const JacobiArgs& a, const Tab& G, const float* pc, float* pn,
                               double& es, long long& ec) {
   const Consts& c = a.c;
-  const float4 xi = a.pos[i];
+  const float4 xi = __ldg(a.pos + i);
   const float4 si = a.s4[i];
-  const int cnt = min(a.cnt_ff[i], c.max_ff);
+  const int cnt = min(__ldg(a.cnt_ff + i), c.max_ff);
   const int* nb = a.nbr_ff + ell_index(i, 0, c.max_ff);
   float acc = 0.f;
-  for (int k = 0; k < cnt; ++k) {
-    const int j = nb[k * kWarp];
-    const float4 xj = a.pos[j];
-    const float4 sj = a.s4[j];
+  for_neighbours(nb, cnt, a.pos, a.s4, [&](const float4 xj, const float4 sj) {
     const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
     const float r = sqrtf(dx * dx + dy * dy + dz * dz);
     const float gs = grad_scalar(G, r, c);
     acc += (si.x - sj.x) * (gs * dx) + (si.y - sj.y) * (gs * dy) + (si.z - sj.z) * (gs * dz);
-  }
-  const float4 bv = a.bvec[i];
-  const float4 da = a.dii_aii[i];
+  });
+  const float4 bv = __ldg(a.bvec + i);
+  const float4 da = __ldg(a.dii_aii + i);
   const float p = pc[i];
   const float Ap = si.w + ((acc * c.m + (si.x * bv.x + si.y * bv.y + si.z * bv.z)) + da.w * p);
   // update_p (IISPH.py:534-539)
@@ -82,15 +121,28 @@ __device__ inline void pass_b(int i, const JacobiArgs& a, const float* G, const 
     es += double(fabsf(rp / c.rho0 - 1.0f));
     ec += 1;
   }
-  const float rho = a.rho[i];
+  const float rho = __ldg(a.rho + i);
   pn[i] = pnew;
   a.P4[i] = make_float4(da.x * pnew, da.y * pnew, da.z * pnew, pnew / (rho * rho));
   a.Ap[i] = Ap;
 }
 
+template <class Tab>
+__device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G);
+
 template <bool SMEM>
 __global__ void __launch_bounds__(kJacobiThreads) k_jacobi(JacobiArgs a) {
-  extern __shared__ float s_tab[];
+  extern __shared__ float2 s_pairs[];
+  if (SMEM) {
+    stage_pairs(s_pairs, a.g_table, a.c.sg);
+    jacobi_body(a, PairTable{s_pairs});
+  } else {
+    jacobi_body(a, FlatTable{a.g_table});
+  }
+}
+
+template <class Tab>
+__device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G) {
   __shared__ double s_sum[kJacobiThreads / 32];
   __shared__ long long s_cnt[kJacobiThreads / 32];
   __shared__ double s_avg;
@@ -101,11 +153,6 @@ __global__ void __launch_bounds__(kJacobiThreads) k_jacobi(JacobiArgs a) {
   // state untouched so the host can grow the lists and redo the step.
   if (*(volatile const int*)&a.acc->flags & (SPH_F_FF_OVERFLOW | SPH_F_FB_OVERFLOW)) return;
 
-  const float* G = a.g_table;
-  if (SMEM) {
-    for (int t = threadIdx.x; t < a.c.sg; t += blockDim.x) s_tab[t] = a.g_table[t];
-    G = s_tab;
-  }
   if (threadIdx.x == 0) s_vmax = 0u;
   __syncthreads();
 
@@ -273,7 +320,7 @@ __global__ void __launch_bounds__(kJacobiThreads) k_jacobi(JacobiArgs a) {
   }
 }
 
-static size_t jacobi_smem(int sg) { return (sg <= 16384) ? sizeof(float) * size_t(sg) : 0; }
+static size_t jacobi_smem(int sg) { return (sg <= 8192) ? sizeof(float2) * size_t(sg) : 0; }
 
 cudaError_t jacobi_config(int block, int sg, int* blocks_per_sm, size_t* smem_out) {
   const size_t smem = jacobi_smem(sg);
