@@ -244,7 +244,7 @@ def bench_ours(args):
 
     # the same K steps with the other warm-start modes (context for the headline)
     modes = {}
-    for mode in ("zero", "half"):
+    for mode in ("zero", "half", "mlp"):
         if mode == headline:
             modes[mode] = {"steps_per_s": K / (ms / 1000.0), "jacobi_iterations": int(sum(iters))}
             continue
@@ -319,6 +319,7 @@ def bench_ours(args):
                        "preset": PRESET, "warm_start": headline, "parallelism": f"replicas{world}",
                        "l2": "working set > 126 MB L2 (no flush needed)"},
             "warm_start_modes": modes,
+            "speedup_vs_plain": value / (world * modes["zero"]["steps_per_s"]) if modes.get("zero") else None,
             "particle_updates_per_s": value * n,
             "jacobi_iterations_mean": float(np.mean(iters)), "avg_err_max": float(np.max([h["avg_err"] for h in hist])),
             "n_ff_pairs_mean": float(np.mean([h["n_ff_pairs"] for h in hist])),
@@ -347,8 +348,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true", help="only warm-up + K steps (for ncu captures)")
-    ap.add_argument("--warm", choices=["zero", "half", "mlp"], default="zero",
-                    help="warm start of the headline run (zero = the reference's p <- 0)")
+    ap.add_argument("--warm", choices=["zero", "half", "mlp"], default="mlp",
+                    help="warm start of the headline run: mlp = learned (default), zero = the "
+                         "reference's p <- 0, half = 0.5 p_prev")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -45,7 +45,7 @@ extern "C" {
 /* Warm-start modes for the pressure solve (IISPH.py:166-174). */
 #define SPH_WARM_ZERO 0 /* p <- 0, the reference's behaviour (IISPH.py:173) */
 #define SPH_WARM_HALF 1 /* p <- 0.5 p_prev (the variant at IISPH.py:174) */
-#define SPH_WARM_MLP 2  /* p <- learned per-particle MLP prediction */
+#define SPH_WARM_MLP 2  /* first iterate <- learned per-particle MLP prediction */
 
 typedef struct SphParams {
   double spacing;    /* DIAMETER (wp_sph/main.py:26) */
@@ -183,6 +183,49 @@ int sph_set_dt(SphCtx* ctx, double dt, double inv_dt);
 #define SPH_NOALLOC_MAX_CELLS 1048576
 int sph_boundary_psi_noalloc(const SphParams* params, const float* d_xb3, int64_t nb, const float* d_w_table,
                              float* d_psi, void* stream);
+
+/* ---- Learned pressure warm start (SPH_WARM_MLP) -------------------------
+ * No counterpart in the reference, whose solve starts from p = 0
+ * (IISPH.py:166-174).  A per-particle MLP 10 -> 64 -> 64 -> 1 (ReLU, BF16
+ * tensor-core products, FP32 accumulate) predicts the solve's starting
+ * pressure from SPH_MLP_FEATURES dimensionless inputs the neighbour build
+ * computes and uses it as the solve's first iterate; the unchanged Jacobi
+ * loop (at least 2 iterations, average density error <= eta) still decides
+ * convergence.
+ * Weights travel as one FP32 blob of SPH_MLP_BLOB floats:
+ *   mu[10], sd[10]   input standardisation (x - mu) / sd
+ *   t_scale          output unit: p = sinh(max(y * t_scale, 0)) * rho0 * g * h
+ *   W1[10][64] b1[64] W2[64][64] b2[64] w3[64] b3   (SPH_MLP_PARAMS, W[in][out])
+ * Training targets are t = asinh(p / (rho0 g h)) of the converged pressure
+ * (pressures span orders of magnitude; asinh keeps them on one scale). */
+#define SPH_MLP_FEATURES 10
+#define SPH_MLP_PARAMS 4929
+#define SPH_MLP_BLOB 4950
+
+typedef struct SphMlpTrainConfig {
+  int32_t epochs;
+  int32_t batch;
+  float lr, beta1, beta2, eps; /* Adam */
+  uint32_t seed;               /* minibatch shuffling */
+  int32_t device;
+} SphMlpTrainConfig;
+
+/* Install the network used by SPH_WARM_MLP. */
+int sph_set_mlp(SphCtx* ctx, const float* blob, int32_t n);
+/* Compute the network inputs at every step (needed to collect training data). */
+int sph_set_record_features(SphCtx* ctx, int32_t on);
+/* After a step: per fluid particle (original order) its SPH_MLP_FEATURES inputs
+ * and the training target asinh(p / (rho0 g h)) of its converged pressure. */
+int sph_get_features(SphCtx* ctx, float* feat, float* target);
+/* Train in place: Adam on mean squared error over shuffled minibatches, on the
+ * GPU with the library's own forward/backward kernels.  blob supplies mu, sd,
+ * t_scale and the initial weights; epoch_loss (epochs floats) may be NULL. */
+int sph_mlp_train(const SphMlpTrainConfig* cfg, const float* feat, const float* target, int64_t n, float* blob,
+                  float* epoch_loss);
+/* Network outputs (units of t_scale) and, with target, the gradient of the mean
+ * squared error: grad[SPH_MLP_PARAMS] in blob parameter order, then the loss. */
+int sph_mlp_eval(const float* blob, const float* feat, const float* target, int64_t n, int32_t device,
+                 float* pred, float* grad);
 
 /* ABI self-description, needs no GPU: out[0] = WPSPH_ABI_VERSION,
  * out[1] = sizeof(SphParams), out[2] = sizeof(SphStepStats). */

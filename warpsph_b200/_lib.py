@@ -61,6 +61,17 @@ class SphParams(ctypes.Structure):
     ]
 
 
+class SphMlpTrainConfig(ctypes.Structure):
+    _fields_ = [("epochs", ctypes.c_int32), ("batch", ctypes.c_int32), ("lr", ctypes.c_float),
+                ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float),
+                ("seed", ctypes.c_uint32), ("device", ctypes.c_int32)]
+
+
+SPH_MLP_FEATURES = 10
+SPH_MLP_PARAMS = 4929
+SPH_MLP_BLOB = 4950
+
+
 class SphStepStats(ctypes.Structure):
     _fields_ = [
         ("iterations", ctypes.c_int32), ("flags", ctypes.c_int32), ("avg_err", ctypes.c_double),
@@ -100,6 +111,11 @@ SIGNATURES = {
     "sph_get_stats": (ctypes.c_int, [_P, ctypes.POINTER(SphStepStats)]),
     "sph_set_dt": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double]),
     "sph_abi_info": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "sph_set_mlp": (ctypes.c_int, [_P, _P, ctypes.c_int32]),
+    "sph_set_record_features": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "sph_get_features": (ctypes.c_int, [_P, _P, _P]),
+    "sph_mlp_train": (ctypes.c_int, [ctypes.POINTER(SphMlpTrainConfig), _P, _P, ctypes.c_int64, _P, _P]),
+    "sph_mlp_eval": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, ctypes.c_int32, _P, _P]),
     "sph_boundary_psi_noalloc": (ctypes.c_int, [ctypes.POINTER(SphParams), _P, ctypes.c_int64, _P, _P, _P]),
     "sph_num_fluid": (ctypes.c_int64, [_P]),
     "sph_num_boundary": (ctypes.c_int64, [_P]),

@@ -182,38 +182,42 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Tab& W, con
     } else if (c.warm_start == SPH_WARM_HALF) {
       p = a.pprev[i] / 2.0f;
     } else {
-      p = fmaxf(a.pmlp[i], 0.f);
+      p = 0.f;  // the learned warm start writes p_0 and P4 after the build
     }
 
     a.rho[i] = rho;
     a.bvec[i] = make_float4(Bx, By, Bz, rho_adv);
     a.dii_aii[i] = make_float4(dix, diy, diz, aii);
     a.vadv[i] = make_float4(vax, vay, vaz, 0.f);
-    a.p0[i] = p;
-    a.P4[i] = make_float4(dix * p, diy * p, diz * p, p / rr);
+    if (c.warm_start != SPH_WARM_MLP) {
+      a.p0[i] = p;
+      a.P4[i] = make_float4(dix * p, diy * p, diz * p, p / rr);
+    }
     a.cnt_ff[i] = cnt;
     if (a.cnt_fb) a.cnt_fb[i] = cntb;
 
     if (a.feat) {
-      // Warm-start MLP features (10 per particle), all O(1) after normalisation.
-      float* f = a.feat + (long long)i * 10;
+      // Learned warm-start inputs (kFeatures per particle, dimensionless; the
+      // network standardises them with its own mean / std).  Pressures span
+      // orders of magnitude, so they enter as asinh(p / (rho0 g h)).
+      float* f = a.feat + (long long)i * kFeatures;
       const float inv_rho0 = 1.0f / c.rho0;
-      const float dv = div * c.m + divb;                // d(rho)/dt from advection
+      const float p_ref = 1.0f / (c.rho0 * c.gravity * c.h);  // 1 / (rho0 g h)
+      const float h2 = c.h * c.h, h4 = h2 * h2;
       float aa = aii;
       if (aa > -c.inv_small && aa < c.inv_small) aa = (aa < 0.f ? -1.f : 1.f) * c.inv_small;
-      const float src = (c.rho0 - rho_adv) / aa;          // unrelaxed first Jacobi guess
-      const float gmag = sqrtf(sGx * sGx + sGy * sGy + sGz * sGz) * c.m * inv_rho0 * (2.0f * c.h);
-      const float pscale = 1.0f / (c.rho0 * c.gravity * c.h * 10.0f);
-      f[0] = (rho_adv - c.rho0) * inv_rho0 * 100.0f;     // predicted density deviation (%)
-      f[1] = dv * inv_rho0 * dt * 100.0f;                 // velocity divergence, % per step
-      f[2] = aii / (t3 / rr * c.m) * 1e-2f;               // a_ii relative to its lattice scale
-      f[3] = ((c.warm_start == SPH_WARM_MLP && a.pprev) ? a.pprev[i] : 0.f) * pscale;  // previous pressure
-      f[4] = float(cnt) * (1.0f / 32.0f);                 // neighbour count
-      f[5] = sWb * inv_rho0;                              // boundary psi sum (boundary density share)
-      f[6] = gmag;                                        // |grad rho| proxy
-      f[7] = src * pscale;                                // Jacobi source term
-      f[8] = (rho - c.rho0) * inv_rho0 * 100.0f;          // current density deviation (%)
-      f[9] = float(cntb) * (1.0f / 32.0f);                // boundary neighbour count
+      const float p1 = fmaxf((c.rho0 - rho_adv) * c.omega / aa, 0.f);  // first Jacobi iterate from p = 0
+      const float gx = sGx * c.m + Bx, gy = sGy * c.m + By, gz = sGz * c.m + Bz;  // grad rho
+      f[0] = rho_adv * inv_rho0 - 1.0f;                        // predicted density deviation
+      f[1] = (rho_adv - rho) * inv_rho0;                       // velocity divergence over the step
+      f[2] = aii * rr / (dt2 * c.m * c.m) * h4 * h4;           // a_ii in lattice units
+      f[3] = asinhf((a.pprev ? a.pprev[i] : 0.f) * p_ref);     // previous-step pressure
+      f[4] = float(cnt);                                       // fluid neighbour count
+      f[5] = sWb * inv_rho0;                                   // boundary psi sum (density share)
+      f[6] = sqrtf(gx * gx + gy * gy + gz * gz) * c.h * inv_rho0;  // |grad rho|
+      f[7] = asinhf(p1 * p_ref);                               // Jacobi source term
+      f[8] = gy * c.h * inv_rho0;                              // grad rho along gravity
+      f[9] = float(cntb);                                      // boundary neighbour count
     }
   }
   // bookkeeping: overflow flags, pair totals, max counts

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "sph_internal.cuh"
+#include "sph_mlp.cuh"
 
 using sph::Consts;
 using sph::DevState;
@@ -52,6 +53,10 @@ struct SphCtx {
   float4 *bvec = nullptr, *dii_aii = nullptr, *vadv = nullptr, *P4 = nullptr, *s4 = nullptr;
   float *p_a = nullptr, *p_b = nullptr, *Ap = nullptr;
   float* pmlp = nullptr;
+  float* feat = nullptr;             // learned warm-start inputs, kFeatures per particle
+  sph::MlpPacked* mlp = nullptr;     // packed network weights
+  bool have_mlp = false;
+  bool record_feat = false;
   float* stage = nullptr;  // 7 floats per particle: host<->device exchange
 
   sph::Partial* partials = nullptr;
@@ -340,6 +345,7 @@ int alloc_fluid(SphCtx* ctx, int64_t n) {
   CK(dalloc(ctx->Ap, m));
   CK(dalloc(ctx->pmlp, m));
   CK(dalloc(ctx->stage, 7 * m));
+  CK(dalloc(ctx->feat, size_t(sph::kFeatures) * m));
   CK(cudaMemset(ctx->rho, 0, sizeof(float) * m));
   CK(cudaMemset(ctx->bvec, 0, sizeof(float4) * m));
   CK(cudaMemset(ctx->dii_aii, 0, sizeof(float4) * m));
@@ -396,7 +402,7 @@ sph::BuildArgs build_args(SphCtx* ctx) {
   b.vadv = ctx->vadv;
   b.p0 = ctx->p_a;
   b.P4 = ctx->P4;
-  b.feat = nullptr;
+  b.feat = (ctx->record_feat || ctx->P.warm_start == SPH_WARM_MLP) ? ctx->feat : nullptr;
   return b;
 }
 
@@ -412,6 +418,18 @@ int enqueue_front(SphCtx* ctx) {
 }
 
 int enqueue_solve(SphCtx* ctx) {
+  if (ctx->P.warm_start == SPH_WARM_MLP) {
+    sph::MlpInferArgs m{};
+    m.n = ctx->n;
+    m.w = ctx->mlp;
+    m.feat = ctx->feat;
+    m.dii_aii = ctx->dii_aii;
+    m.rho = ctx->rho;
+    m.p_unit = float(ctx->P.rho0 * ctx->P.gravity * ctx->P.h);
+    m.p0 = ctx->p_a;
+    m.P4 = ctx->P4;
+    CK(sph::launch_mlp_infer(m, ctx->sm_count, ctx->stream));
+  }
   sph::JacobiArgs j{};
   j.n = int(ctx->n);
   j.c = ctx->c;
@@ -438,7 +456,10 @@ int enqueue_solve(SphCtx* ctx) {
   j.vel_out = ctx->vel_s;
   j.orig_out = ctx->orig_s;
   j.p_out = ctx->p_s;
-  j.start_iter = (ctx->P.warm_start == SPH_WARM_ZERO) ? 1 : 0;
+  // p_1 comes from the build (zero start: p_0 = 0 makes the first update local)
+  // or from the network (its prediction is used as the first iterate); the
+  // 0.5 p_prev start runs the reference's extra Ap_0 evaluation (pass 0).
+  j.start_iter = (ctx->P.warm_start == SPH_WARM_HALF) ? 0 : 1;
   j.budget = (long long)ctx->P.timeout_ms * (long long)ctx->clock_khz;
   j.dt_max = ctx->P.dt_max;
   j.cfl_len = ctx->P.cfl_len;
@@ -455,6 +476,8 @@ int enqueue_step(SphCtx* ctx) {
 }
 
 int ensure_ready(SphCtx* ctx) {
+  if (ctx->P.warm_start == SPH_WARM_MLP && !ctx->have_mlp)
+    return fail(ctx, SPH_E_INVALID, "SPH_WARM_MLP needs a network: call sph_set_mlp first");
   if (!ctx->grid_valid) {
     int rc = set_grid(ctx, nullptr, 0);
     if (rc < 0) return rc;
@@ -633,7 +656,7 @@ void sph_destroy(SphCtx* ctx) {
                   ctx->pos_w, ctx->vel_w, ctx->orig_s, ctx->orig_w, ctx->p_s, ctx->pprev_w, ctx->key, ctx->rank,
                   ctx->sort_src, ctx->sort_orig, ctx->cell_count, ctx->cell_start, ctx->scan_part, ctx->nbr_ff,
                   ctx->cnt_ff, ctx->nbr_fb, ctx->cnt_fb, ctx->rho, ctx->bvec, ctx->dii_aii, ctx->vadv, ctx->P4,
-                  ctx->s4, ctx->p_a, ctx->p_b, ctx->Ap, ctx->pmlp, ctx->stage, ctx->partials, ctx->st, ctx->acc, ctx->ring,
+                  ctx->s4, ctx->p_a, ctx->p_b, ctx->Ap, ctx->pmlp, ctx->feat, ctx->mlp, ctx->stage, ctx->partials, ctx->st, ctx->acc, ctx->ring,
                   ctx->last};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -977,6 +1000,58 @@ int sph_get_neighbors(SphCtx* ctx, int64_t* ff_off, int32_t* ff_idx, int64_t ff_
     if (ctx->nb) CK(cudaMemcpy(bo.data(), ctx->borig, sizeof(int) * ctx->nb, cudaMemcpyDeviceToHost));
     int rc = export_lists(ctx->nbr_fb, ctx->cnt_fb, ctx->K_fb, bo.data(), fb_off, fb_idx, fb_cap);
     if (rc) return rc;
+  }
+  return SPH_OK;
+}
+
+int sph_set_mlp(SphCtx* ctx, const float* blob, int32_t n) {
+  if (!ctx || !blob || n != SPH_MLP_BLOB) return fail(ctx, SPH_E_INVALID, "the network blob has SPH_MLP_BLOB floats");
+  for (int c = 0; c < sph::kFeatures; ++c)
+    if (!(blob[sph::kBlobSd + c] > 0)) return fail(ctx, SPH_E_INVALID, "input scales must be positive");
+  CK(cudaSetDevice(ctx->dev));
+  CK(cudaStreamSynchronize(ctx->stream));
+  float* d_blob = nullptr;
+  CK(dalloc(d_blob, SPH_MLP_BLOB));
+  cudaError_t e = cudaMemcpy(d_blob, blob, sizeof(float) * SPH_MLP_BLOB, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !ctx->mlp) e = cudaMalloc(&ctx->mlp, sizeof(sph::MlpPacked));
+  if (e == cudaSuccess) e = sph::launch_mlp_pack(d_blob, ctx->mlp, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d_blob);
+  if (e != cudaSuccess) return fail(ctx, SPH_E_CUDA, std::string("sph_set_mlp: ") + cudaGetErrorString(e));
+  ctx->have_mlp = true;
+  return SPH_OK;
+}
+
+int sph_set_record_features(SphCtx* ctx, int32_t on) {
+  if (!ctx) return SPH_E_INVALID;
+  if (ctx->record_feat != (on != 0)) ctx->graph_dirty = true;
+  ctx->record_feat = (on != 0);
+  return SPH_OK;
+}
+
+int sph_get_features(SphCtx* ctx, float* feat, float* target) {
+  if (!ctx) return SPH_E_INVALID;
+  if (!ctx->record_feat && ctx->P.warm_start != SPH_WARM_MLP)
+    return fail(ctx, SPH_E_INVALID, "features are only computed with sph_set_record_features(ctx, 1)");
+  CK(cudaSetDevice(ctx->dev));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const int64_t n = ctx->n;
+  if (n == 0) return SPH_OK;
+  std::vector<int> ow(n);
+  CK(cudaMemcpy(ow.data(), ctx->orig_w, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  if (feat) {
+    std::vector<float> h(size_t(n) * sph::kFeatures);
+    CK(cudaMemcpy(h.data(), ctx->feat, sizeof(float) * h.size(), cudaMemcpyDeviceToHost));
+    for (int64_t k = 0; k < n; ++k)
+      std::memcpy(feat + size_t(ow[k]) * sph::kFeatures, h.data() + size_t(k) * sph::kFeatures,
+                  sizeof(float) * sph::kFeatures);
+  }
+  if (target) {
+    // the last step's converged pressure, in the state order of that step (= orig_w)
+    std::vector<float> h(n);
+    CK(cudaMemcpy(h.data(), ctx->p_s, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    const double unit = 1.0 / (ctx->P.rho0 * ctx->P.gravity * ctx->P.h);
+    for (int64_t k = 0; k < n; ++k) target[ow[k]] = float(std::asinh(double(h[k]) * unit));
   }
   return SPH_OK;
 }

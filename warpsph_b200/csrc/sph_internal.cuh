@@ -16,6 +16,7 @@
 namespace sph {
 
 constexpr int kWarp = 32;
+constexpr int kFeatures = 10;  // learned warm-start inputs per particle
 
 // Uniform neighbour grid.  Cell size is slightly above h, so every neighbour
 // within h of a particle lies in the 3x3x3 cells around it even after float32

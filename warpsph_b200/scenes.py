@@ -107,3 +107,23 @@ def preset_scene(name: str) -> Scene:
     c = PRESETS[name]
     return dam_break(fluid=c["fluid"], spacing=c["diameter"], box=c["box"], jitter=c["jitter"],
                      layers=c["layers"], seed=c["seed"])
+
+
+def batched_scenes(count=64, seed=3, spacing=0.01, jitter=5e-5, layers=2):
+    """Independent dam breaks for batched solving: fluid counts log-uniform in
+    [5k, 200k], box aspect ratios uniform in [1, 3] per axis, fluid fill
+    fraction uniform in [0.2, 0.5] (seeded).  The fluid block sits in the box
+    corner with the box's proportions scaled by fill^(1/3)."""
+    rng = np.random.default_rng(seed)
+    scenes = []
+    for k in range(count):
+        n_target = float(np.exp(rng.uniform(np.log(5e3), np.log(2e5))))
+        aspect = rng.uniform(1.0, 3.0, size=3)
+        fill = float(rng.uniform(0.2, 0.5))
+        v_box = n_target * spacing**3 / fill
+        box = aspect * (v_box / float(np.prod(aspect))) ** (1.0 / 3.0)
+        nf = [max(2, int(round(fill ** (1.0 / 3.0) * b / spacing))) for b in box]
+        box = tuple(float(max(b, (n + 1) * spacing)) for b, n in zip(box, nf))
+        scenes.append(dam_break(fluid=tuple(nf), spacing=spacing, box=box, jitter=jitter, layers=layers,
+                                seed=seed * 1000 + k))
+    return scenes

@@ -175,7 +175,16 @@ class IISPH:
         self._ctx = ctx
         w, g = kernel_tables(self.params)
         _lib.check(ctx, self._lib.sph_set_tables(ctx, _lib.ptr(w), len(w), _lib.ptr(g), len(g)))
+        if self.params.warm_start == "mlp":
+            self.set_mlp(self.params.extra.get("mlp_blob"))
         self._upload()
+
+    def set_mlp(self, blob=None):
+        """Install the learned warm-start network (default: the shipped weights)."""
+        from .learned import load_blob
+
+        blob = load_blob() if blob is None else np.ascontiguousarray(blob, dtype=np.float32)
+        _lib.check(self._ctx, self._lib.sph_set_mlp(self._ctx, _lib.ptr(blob), len(blob)))
 
     def _upload(self):
         s = self._scene

@@ -1,0 +1,50 @@
+"""Train the shipped learned warm-start network (GPU).
+
+    python -m warpsph_b200.train_warm_start [--pairs 2000000] [--steps 400] [--epochs 20]
+
+Data: the solver's own converged pressures on the 64 batched dam-break scenes
+(`scenes.batched_scenes`, 0.01 m spacing, dt 5e-4, 1024-sample tables,
+g = 9.81), `--steps` steps each, sampled evenly to `--pairs` pairs.  Training:
+Adam, lr 1e-3, MSE, on the GPU with libwpsph's own kernels.  Output:
+warpsph_b200/data/warm_start_mlp.npz.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import learned
+from .params import SolverParams
+from .scenes import batched_scenes
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--pairs", type=int, default=2_000_000)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--scenes", type=int, default=64)
+    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--out", default=str(learned.DEFAULT_WEIGHTS))
+    ap.add_argument("--seed", type=int, default=0)
+    a = ap.parse_args()
+    scenes = batched_scenes(count=a.scenes)
+    per_step = max(1, a.pairs // (a.scenes * a.steps))
+    t0 = time.time()
+    params = SolverParams(diameter=0.01, gravity=9.81, w_table_size=1024, g_table_size=1024)
+    feat, target = learned.collect(scenes, a.steps, per_step, lambda sc: params, seed=a.seed)
+    t1 = time.time()
+    blob, losses = learned.train(feat, target, epochs=a.epochs, lr=a.lr, seed=a.seed)
+    t2 = time.time()
+    meta = dict(pairs=len(target), scenes=a.scenes, steps=a.steps, epochs=a.epochs, lr=a.lr,
+                losses=losses.tolist(), collect_s=t1 - t0, train_s=t2 - t1)
+    learned.save(a.out, blob, meta=json.dumps(meta))
+    print(json.dumps(meta))
+
+
+if __name__ == "__main__":
+    main()
