@@ -73,12 +73,15 @@ typedef struct SphParams {
   int32_t keep_fb_lists; /* unused (fluid-boundary lists are always kept); must be 0 or 1 */
   int32_t use_graph;     /* replay the step as a CUDA graph */
   int32_t device;        /* CUDA device ordinal */
-  int32_t block_size;    /* threads per block for particle kernels (0 = auto) */
+  int32_t block_size;    /* threads per block of the neighbour build (0 = 128) */
   int32_t timeout_ms;    /* bound on every grid-wide wait */
-  int32_t reserved[5];
+  int32_t jacobi_block;  /* threads per block of the pressure solve: 128 or 256 (0 = 256) */
+  int32_t jacobi_ppt;    /* particles per solve thread: 1 or 2 (0 = 1) */
+  int32_t jacobi_unroll; /* neighbour-loop unroll of the solve: 2, 4 or 8 (0 = 4) */
+  int32_t reserved[2];
 } SphParams;
 
-typedef struct SphStepStats {
+typedef struct SphStepStats { /* for a batch: max over scenes, dt and time of scene 0 */
   int32_t iterations; /* Jacobi iterations executed (IISPH.py:1200-1296 `loop`) */
   int32_t flags;      /* SPH_F_* */
   double avg_err;     /* average_rho_error (IISPH.py:1489-1494), FP64 reduction */
@@ -116,6 +119,33 @@ int sph_set_boundary(SphCtx* ctx, const float* xb3, const float* vb3, int64_t nb
 
 /* Fluid particles (IISPH.py:993-994) with velocities (NULL = zero). */
 int sph_set_fluid(SphCtx* ctx, const float* x3, const float* v3, int64_t n);
+
+/* ---- Batches of independent scenes ---------------------------------------
+ * No counterpart in the reference (one scene per IISPH object).  All scenes
+ * share the physical parameters and advance together: one sort, one build and
+ * one persistent solve per step, in which each scene keeps its own grid, dt,
+ * CFL, residual, convergence decision and iteration count; a converged scene
+ * drops out of the remaining Jacobi passes.  Fluid and boundary arrays of the
+ * batch are the scenes' arrays concatenated in scene order (sph_set_fluid,
+ * sph_get_fluid, ... then take and return those concatenations). */
+typedef struct SphSceneDesc {
+  const float* x3;  /* n x 3 fluid positions */
+  const float* v3;  /* n x 3 fluid velocities, NULL = zero */
+  int64_t n;
+  const float* xb3; /* nb x 3 boundary positions */
+  const float* vb3; /* NULL = static */
+  int64_t nb;
+  double domain_min[3], domain_max[3]; /* grid extent; zero extent = fit to the particles */
+} SphSceneDesc;
+
+int sph_create_batch(const SphParams* params, const SphSceneDesc* scenes, int32_t nscenes, SphCtx** out);
+int32_t sph_num_scenes(const SphCtx* ctx);
+/* fluid_off / boundary_off: nscenes + 1 prefix offsets into the concatenated arrays. */
+int sph_get_scene_ranges(SphCtx* ctx, int64_t* fluid_off, int64_t* boundary_off);
+/* Per-scene results of the last step (arrays of nscenes; any may be NULL):
+ * Jacobi iterations, average density error, max |v|, next dt, simulated time. */
+int sph_get_scene_stats(SphCtx* ctx, int32_t* iterations, double* avg_err, double* v_max, double* dt,
+                        double* sim_time);
 
 /* Pressure carried into the next step's warm start (SPH_WARM_HALF / SPH_WARM_MLP). */
 int sph_set_pressure(SphCtx* ctx, const float* p, int64_t n);

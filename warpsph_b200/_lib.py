@@ -57,7 +57,8 @@ class SphParams(ctypes.Structure):
         ("max_loop", ctypes.c_int32), ("fixed_iters", ctypes.c_int32), ("warm_start", ctypes.c_int32),
         ("max_ff", ctypes.c_int32), ("max_fb", ctypes.c_int32), ("keep_fb_lists", ctypes.c_int32),
         ("use_graph", ctypes.c_int32), ("device", ctypes.c_int32), ("block_size", ctypes.c_int32),
-        ("timeout_ms", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5),
+        ("timeout_ms", ctypes.c_int32), ("jacobi_block", ctypes.c_int32), ("jacobi_ppt", ctypes.c_int32),
+        ("jacobi_unroll", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2),
     ]
 
 
@@ -70,6 +71,12 @@ class SphMlpTrainConfig(ctypes.Structure):
 SPH_MLP_FEATURES = 10
 SPH_MLP_PARAMS = 4929
 SPH_MLP_BLOB = 4950
+
+
+class SphSceneDesc(ctypes.Structure):
+    _fields_ = [("x3", ctypes.c_void_p), ("v3", ctypes.c_void_p), ("n", ctypes.c_int64),
+                ("xb3", ctypes.c_void_p), ("vb3", ctypes.c_void_p), ("nb", ctypes.c_int64),
+                ("domain_min", ctypes.c_double * 3), ("domain_max", ctypes.c_double * 3)]
 
 
 class SphStepStats(ctypes.Structure):
@@ -111,6 +118,10 @@ SIGNATURES = {
     "sph_get_stats": (ctypes.c_int, [_P, ctypes.POINTER(SphStepStats)]),
     "sph_set_dt": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double]),
     "sph_abi_info": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "sph_create_batch": (ctypes.c_int, [ctypes.POINTER(SphParams), _P, ctypes.c_int32, ctypes.POINTER(_P)]),
+    "sph_num_scenes": (ctypes.c_int32, [_P]),
+    "sph_get_scene_ranges": (ctypes.c_int, [_P, _P, _P]),
+    "sph_get_scene_stats": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),
     "sph_set_mlp": (ctypes.c_int, [_P, _P, ctypes.c_int32]),
     "sph_set_record_features": (ctypes.c_int, [_P, ctypes.c_int32]),
     "sph_get_features": (ctypes.c_int, [_P, _P, _P]),

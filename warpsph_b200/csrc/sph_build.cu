@@ -29,14 +29,14 @@ namespace sph {
 // rows of 3 x-adjacent cells with the exact float32 test and write the hits
 // into the particle's ELL list.  Only a compare and a predicated store run per
 // candidate, so the warp stays converged; loads are issued four at a time.
-__device__ inline int filter_rows(const Grid& g, int3 ci, const int* __restrict__ cell_start,
+__device__ inline int filter_rows(const Grid& g, int base, int3 ci, const int* __restrict__ cell_start,
                                   const float4* __restrict__ pts, float4 xi, float r2_limit, int self, int* out,
                                   int K) {
   int cnt = 0;
   const int x0 = max(ci.x - 1, 0), x1 = min(ci.x + 1, g.nx - 1);
   for (int cz = max(ci.z - 1, 0); cz <= min(ci.z + 1, g.nz - 1); ++cz) {
     for (int cy = max(ci.y - 1, 0); cy <= min(ci.y + 1, g.ny - 1); ++cy) {
-      const int row = (cz * g.ny + cy) * g.nx;
+      const int row = base + (cz * g.ny + cy) * g.nx;
       const int jb = __ldg(cell_start + row + x0), je = __ldg(cell_start + row + x1 + 1);
       int j = jb;
       for (; j + 4 <= je; j += 4) {
@@ -84,12 +84,13 @@ __global__ void __launch_bounds__(256) k_build(BuildArgs a) {
 template <class Tab>
 __device__ __forceinline__ void build_body(const BuildArgs& a, const Tab& W, const Tab& G) {
   const Consts c = a.c;
-  const Grid g = a.grid;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = i < a.n;
   int cnt = 0, cntb = 0;
   if (live) {
-    const float dt = a.st->dt;
+    const CellFrame fr = frame_of(a.scenes, a.grid, false, i);
+    const Grid& g = fr.g;
+    const float dt = a.st->dt[fr.scene];
     const float gdt = (-c.gravity) * dt;
     const float4 xi = a.pos[i];
     const float4 vi = a.vel[i];
@@ -100,8 +101,8 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Tab& W, con
     int* nbrb = a.nbr_fb + ell_index(i, 0, KB);
 
     // phase 1: neighbour lists
-    cnt = filter_rows(g, ci, a.cell_start, a.pos, xi, c.r2_limit, i, nbr, K);
-    if (a.nb > 0) cntb = filter_rows(g, ci, a.bcell_start, a.bpos, xi, c.r2_limit, -1, nbrb, KB);
+    cnt = filter_rows(g, fr.base, ci, a.cell_start, a.pos, xi, c.r2_limit, i, nbr, K);
+    if (a.nb > 0) cntb = filter_rows(g, fr.base, ci, a.bcell_start, a.bpos, xi, c.r2_limit, -1, nbrb, KB);
 
     // phase 2: everything summed over the neighbours, in list (= ascending j) order
     float sW = 0.f, sGx = 0.f, sGy = 0.f, sGz = 0.f, sG2 = 0.f, div = 0.f;
@@ -241,14 +242,15 @@ __global__ void __launch_bounds__(256) k_psi(PsiArgs a, float* psi) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= a.nb) return;
   const Consts c = a.c;
-  const Grid g = a.grid;
+  const CellFrame fr = frame_of(a.scenes, a.grid, true, b);
+  const Grid& g = fr.g;
   const float4 xb = a.bpos[b];
   const int3 ci = cell_coord(g, xb.x, xb.y, xb.z);
   float rho = c.w0;
   const int x0 = max(ci.x - 1, 0), x1 = min(ci.x + 1, g.nx - 1);
   for (int cz = max(ci.z - 1, 0); cz <= min(ci.z + 1, g.nz - 1); ++cz)
     for (int cy = max(ci.y - 1, 0); cy <= min(ci.y + 1, g.ny - 1); ++cy) {
-      const int row = (cz * g.ny + cy) * g.nx;
+      const int row = fr.base + (cz * g.ny + cy) * g.nx;
       for (int j = a.bcell_start[row + x0]; j < a.bcell_start[row + x1 + 1]; ++j) {
         if (j == b) continue;
         const float4 xj = a.bpos[j];

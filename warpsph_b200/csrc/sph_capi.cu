@@ -23,9 +23,20 @@ struct SphCtx {
   int sm_count = 0;
   int clock_khz = 0;
   Consts c{};
-  Grid grid{};
   bool grid_valid = false;
   int ncells_cap = 0;
+
+  // scenes (a single scene is nscenes = 1)
+  int S = 1;
+  std::vector<int64_t> f_off{0, 0}, b_off{0, 0};  // host prefix offsets of fluid / boundary slots
+  std::vector<Grid> grids;                        // per scene
+  std::vector<int> cell_base;                     // prefix of per-scene cell counts
+  std::vector<double> domains;                    // 6 per scene (min xyz, max xyz); zero extent = fit
+  int total_cells = 0;
+  sph::SceneTable* d_scenes = nullptr;
+  int2* d_chunks = nullptr;
+  int* d_chunk_scene = nullptr;
+  int nchunks = 0;
 
   std::vector<float> w_host, g_host;
   float* d_w = nullptr;
@@ -59,10 +70,13 @@ struct SphCtx {
   bool record_feat = false;
   float* stage = nullptr;  // 7 floats per particle: host<->device exchange
 
-  sph::Partial* partials = nullptr;
+  sph::Partial* partials = nullptr;  // [cooperative block][scene]
+  int64_t partials_cap = 0;
   int coop_grid = 0;
   int blocks_per_sm = 0;
   size_t jac_smem = 0;
+  int jac_block = 256, jac_ppt = 1, jac_unroll = 4;  // autotuner knobs of the solve
+  int chunk = 256;                                    // particles per solve chunk
 
   DevState* st = nullptr;
   StepAcc* acc = nullptr;
@@ -175,38 +189,11 @@ int upload_tables(SphCtx* ctx) {
   return SPH_OK;
 }
 
-// Grid over the union of boundary and fluid bounding boxes (or params.domain),
-// padded by 2h, cell size 1.01 h (grown if the cell count would exceed 2^26).
-int set_grid(SphCtx* ctx, const float* xf, int64_t n) {
-  double lo[3], hi[3];
-  const SphParams& P = ctx->P;
-  bool have_domain = false;
-  for (int a = 0; a < 3; ++a) have_domain = have_domain || (P.domain_max[a] > P.domain_min[a]);
-  if (have_domain) {
-    for (int a = 0; a < 3; ++a) {
-      lo[a] = P.domain_min[a];
-      hi[a] = P.domain_max[a];
-    }
-  } else {
-    for (int a = 0; a < 3; ++a) {
-      lo[a] = 1e300;
-      hi[a] = -1e300;
-    }
-    auto fold = [&](const float* x, int64_t m) {
-      for (int64_t i = 0; i < m; ++i)
-        for (int a = 0; a < 3; ++a) {
-          const double v = x[3 * i + a];
-          if (std::isfinite(v)) {
-            lo[a] = std::min(lo[a], v);
-            hi[a] = std::max(hi[a], v);
-          }
-        }
-    };
-    fold(ctx->bx_host.data(), ctx->nb);
-    if (xf) fold(xf, n);
-    for (int a = 0; a < 3; ++a)
-      if (lo[a] > hi[a]) lo[a] = hi[a] = 0.0;
-  }
+// One grid per scene over the union of its boundary and fluid bounding boxes
+// (or its domain), padded by 2h, cell size 1.01 h (grown if a scene's cell count
+// would exceed 2^26).  Scenes get consecutive global cell-id ranges.  Returns 1
+// when any grid changed, 0 when none did, < 0 on error.
+Grid fit_grid(const SphParams& P, const double* lo, const double* hi) {
   double cell = double(float(P.h)) * 1.01;
   const double pad = 2.0 * P.h;
   long long dims[3];
@@ -228,16 +215,108 @@ int set_grid(SphCtx* ctx, const float* xf, int64_t n) {
   g.ny = int(dims[1]);
   g.nz = int(dims[2]);
   g.ncells = int(dims[0] * dims[1] * dims[2]);
-  const bool changed = !ctx->grid_valid || std::memcmp(&g, &ctx->grid, sizeof(Grid)) != 0;
-  ctx->grid = g;
-  ctx->grid_valid = true;
-  if (g.ncells > ctx->ncells_cap) {
-    CK(dalloc(ctx->cell_count, g.ncells));
-    CK(dalloc(ctx->cell_start, g.ncells + 1));
-    CK(dalloc(ctx->bcell_start, g.ncells + 1));
-    CK(dalloc(ctx->scan_part, g.ncells / 4096 + 2));
-    ctx->ncells_cap = g.ncells;
+  return g;
+}
+
+int upload_scene_table(SphCtx* ctx) {
+  const int S = ctx->S;
+  // scene-aligned chunks of at most kChunk fluid slots
+  std::vector<int2> chunks;
+  std::vector<int> cscene;
+  sph::SceneTable T{};
+  T.nscenes = S;
+  for (int sc = 0; sc < S; ++sc) {
+    T.chunk_off[sc] = int(chunks.size());
+    for (int64_t a = ctx->f_off[sc]; a < ctx->f_off[sc + 1]; a += ctx->chunk) {
+      chunks.push_back(make_int2(int(a), int(std::min<int64_t>(a + ctx->chunk, ctx->f_off[sc + 1]))));
+      cscene.push_back(sc);
+    }
   }
+  T.chunk_off[S] = int(chunks.size());
+  for (int sc = 0; sc <= S; ++sc) {
+    T.cell_base[sc] = ctx->cell_base[sc];
+    T.fluid_off[sc] = int(ctx->f_off[sc]);
+    T.bound_off[sc] = int(ctx->b_off[sc]);
+  }
+  for (int sc = 0; sc < S; ++sc) T.grid[sc] = ctx->grids[sc];
+  if (!ctx->d_scenes) CK(cudaMalloc(&ctx->d_scenes, sizeof(sph::SceneTable)));
+  CK(cudaMemcpy(ctx->d_scenes, &T, sizeof(T), cudaMemcpyHostToDevice));
+  if (int(chunks.size()) != ctx->nchunks || !ctx->d_chunks) {
+    ctx->nchunks = int(chunks.size());
+    CK(dalloc(ctx->d_chunks, chunks.size()));
+    CK(dalloc(ctx->d_chunk_scene, chunks.size()));
+  }
+  if (!chunks.empty()) {
+    CK(cudaMemcpy(ctx->d_chunks, chunks.data(), sizeof(int2) * chunks.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_chunk_scene, cscene.data(), sizeof(int) * cscene.size(), cudaMemcpyHostToDevice));
+  }
+  ctx->graph_dirty = true;
+  return SPH_OK;
+}
+
+int set_grid(SphCtx* ctx, const float* xf, int64_t n) {
+  const SphParams& P = ctx->P;
+  const int S = ctx->S;
+  std::vector<Grid> grids(S);
+  for (int sc = 0; sc < S; ++sc) {
+    double lo[3], hi[3];
+    const double* dom = ctx->domains.empty() ? nullptr : &ctx->domains[6 * size_t(sc)];
+    bool have_domain = false;
+    for (int a = 0; a < 3; ++a) {
+      const double dmin = dom ? dom[a] : P.domain_min[a], dmax = dom ? dom[3 + a] : P.domain_max[a];
+      have_domain = have_domain || (dmax > dmin);
+    }
+    if (have_domain) {
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = dom ? dom[a] : P.domain_min[a];
+        hi[a] = dom ? dom[3 + a] : P.domain_max[a];
+      }
+    } else {
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = 1e300;
+        hi[a] = -1e300;
+      }
+      auto fold = [&](const float* x, int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i)
+          for (int a = 0; a < 3; ++a) {
+            const double v = x[3 * i + a];
+            if (std::isfinite(v)) {
+              lo[a] = std::min(lo[a], v);
+              hi[a] = std::max(hi[a], v);
+            }
+          }
+      };
+      if (ctx->nb) fold(ctx->bx_host.data(), ctx->b_off[sc], ctx->b_off[sc + 1]);
+      if (xf && n == ctx->f_off[S]) fold(xf, ctx->f_off[sc], ctx->f_off[sc + 1]);
+      for (int a = 0; a < 3; ++a)
+        if (lo[a] > hi[a]) lo[a] = hi[a] = 0.0;
+    }
+    grids[sc] = fit_grid(P, lo, hi);
+  }
+  std::vector<int> base(S + 1, 0);
+  long long total = 0;
+  for (int sc = 0; sc < S; ++sc) {
+    base[sc] = int(total);
+    total += grids[sc].ncells;
+  }
+  if (total > (1ll << 28)) return fail(ctx, SPH_E_INVALID, "too many grid cells in total");
+  base[S] = int(total);
+  bool changed = !ctx->grid_valid || int(ctx->grids.size()) != S;
+  if (!changed)
+    for (int sc = 0; sc < S; ++sc) changed = changed || std::memcmp(&grids[sc], &ctx->grids[sc], sizeof(Grid)) != 0;
+  ctx->grids = grids;
+  ctx->cell_base = base;
+  ctx->total_cells = int(total);
+  ctx->grid_valid = true;
+  if (ctx->total_cells > ctx->ncells_cap) {
+    CK(dalloc(ctx->cell_count, ctx->total_cells));
+    CK(dalloc(ctx->cell_start, ctx->total_cells + 1));
+    CK(dalloc(ctx->bcell_start, ctx->total_cells + 1));
+    CK(dalloc(ctx->scan_part, ctx->total_cells / 4096 + 2));
+    ctx->ncells_cap = ctx->total_cells;
+  }
+  int rc = upload_scene_table(ctx);
+  if (rc) return rc;
   if (changed) ctx->graph_dirty = true;
   return changed ? 1 : 0;
 }
@@ -245,7 +324,7 @@ int set_grid(SphCtx* ctx, const float* xf, int64_t n) {
 // Sort the boundary into the grid and compute psi (compute_boundary_density).
 int sort_boundary(SphCtx* ctx) {
   const int64_t nb = ctx->nb;
-  const int nc = ctx->grid.ncells;
+  const int nc = ctx->total_cells;
   if (nb == 0) {
     CK(cudaMemsetAsync(ctx->bcell_start, 0, sizeof(int) * (nc + 1), ctx->stream));
     return SPH_OK;
@@ -276,7 +355,9 @@ int sort_boundary(SphCtx* ctx) {
   else dfree(ctx->bvel);
   sph::SortArgs s{};
   s.n = int(nb);
-  s.grid = ctx->grid;
+  s.grid = ctx->grids[0];
+  s.scenes = ctx->d_scenes;
+  s.boundary = 1;
   s.pos = tx;
   s.orig = to;
   s.key = key;
@@ -293,7 +374,8 @@ int sort_boundary(SphCtx* ctx) {
                         ctx->stream));
   sph::PsiArgs pa{};
   pa.nb = int(nb);
-  pa.grid = ctx->grid;
+  pa.grid = ctx->grids[0];
+  pa.scenes = ctx->d_scenes;
   pa.c = ctx->c;
   pa.w_table = ctx->d_w;
   pa.bpos = ctx->bpos;
@@ -361,7 +443,8 @@ int alloc_fluid(SphCtx* ctx, int64_t n) {
 sph::SortArgs fluid_sort_args(SphCtx* ctx) {
   sph::SortArgs s{};
   s.n = int(ctx->n);
-  s.grid = ctx->grid;
+  s.grid = ctx->grids[0];
+  s.scenes = ctx->d_scenes;
   s.pos = ctx->pos_s;
   s.orig = ctx->orig_s;
   s.key = ctx->key;
@@ -378,7 +461,8 @@ sph::BuildArgs build_args(SphCtx* ctx) {
   sph::BuildArgs b{};
   b.n = int(ctx->n);
   b.nb = int(ctx->nb);
-  b.grid = ctx->grid;
+  b.grid = ctx->grids[0];
+  b.scenes = ctx->d_scenes;
   b.c = ctx->c;
   b.w_table = ctx->d_w;
   b.g_table = ctx->d_g;
@@ -409,7 +493,7 @@ sph::BuildArgs build_args(SphCtx* ctx) {
 // sort + gather + build: everything up to the pressure solve
 int enqueue_front(SphCtx* ctx) {
   CK(cudaMemsetAsync(ctx->acc, 0, sizeof(StepAcc), ctx->stream));
-  CK(sph::launch_sort(fluid_sort_args(ctx), ctx->grid.ncells, ctx->stream));
+  CK(sph::launch_sort(fluid_sort_args(ctx), ctx->total_cells, ctx->stream));
   CK(sph::launch_gather(int(ctx->n), ctx->sort_src, ctx->sort_orig, ctx->pos_s, ctx->vel_s, ctx->p_s, ctx->pos_w,
                         ctx->vel_w, ctx->orig_w, ctx->pprev_w, ctx->stream));
   int block = ctx->P.block_size > 0 ? ctx->P.block_size : 128;
@@ -432,6 +516,11 @@ int enqueue_solve(SphCtx* ctx) {
   }
   sph::JacobiArgs j{};
   j.n = int(ctx->n);
+  j.nscenes = ctx->S;
+  j.nchunks = ctx->nchunks;
+  j.chunks = ctx->d_chunks;
+  j.chunk_scene = ctx->d_chunk_scene;
+  j.scenes = ctx->d_scenes;
   j.c = ctx->c;
   j.g_table = ctx->d_g;
   j.pos = ctx->pos_w;
@@ -465,7 +554,8 @@ int enqueue_solve(SphCtx* ctx) {
   j.cfl_len = ctx->P.cfl_len;
   j.inv_small_d = ctx->P.inv_small;
   j.eta_d = ctx->P.eta;
-  CK(sph::launch_jacobi(j, ctx->coop_grid, 256, ctx->jac_smem, ctx->stream));
+  CK(sph::launch_jacobi(j, ctx->coop_grid, ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll, ctx->jac_smem,
+                        ctx->stream));
   return SPH_OK;
 }
 
@@ -487,6 +577,12 @@ int ensure_ready(SphCtx* ctx) {
   if (!ctx->pos_s) {
     int rc = alloc_fluid(ctx, 1);
     if (rc) return rc;
+  }
+  const int64_t need = int64_t(ctx->coop_grid) * ctx->S;
+  if (need > ctx->partials_cap) {
+    CK(dalloc(ctx->partials, need));
+    ctx->partials_cap = need;
+    ctx->graph_dirty = true;
   }
   return SPH_OK;
 }
@@ -633,16 +729,23 @@ int sph_create(const SphParams* params, SphCtx** out) {
   cudaMemset(ctx->ring, 0, sizeof(SphStepStats) * sph::kStatsRing);
   cudaMemset(ctx->last, 0, sizeof(SphStepStats));
   DevState s{};
-  s.dt64 = P.dt0;
-  s.inv_dt64 = 1.0 / P.dt0;
-  s.dt = float(s.dt64);
-  s.inv_dt = float(s.inv_dt64);
+  for (int sc = 0; sc < sph::kMaxScenes; ++sc) {
+    s.dt64[sc] = P.dt0;
+    s.inv_dt64[sc] = 1.0 / P.dt0;
+    s.dt[sc] = float(s.dt64[sc]);
+    s.inv_dt[sc] = float(s.inv_dt64[sc]);
+  }
   if (cudaMemcpy(ctx->st, &s, sizeof(s), cudaMemcpyHostToDevice) != cudaSuccess) return bail(SPH_E_CUDA);
-  if (sph::jacobi_config(256, ctx->c.sg, &ctx->blocks_per_sm, &ctx->jac_smem) != cudaSuccess ||
+  ctx->jac_block = P.jacobi_block ? P.jacobi_block : 256;
+  ctx->jac_ppt = P.jacobi_ppt ? P.jacobi_ppt : 1;
+  ctx->jac_unroll = P.jacobi_unroll ? P.jacobi_unroll : 4;
+  if (!sph::jacobi_variant_ok(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll)) return bail(SPH_E_INVALID);
+  ctx->chunk = ctx->jac_block * ctx->jac_ppt;
+  if (sph::jacobi_config(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll, ctx->c.sg, &ctx->blocks_per_sm,
+                         &ctx->jac_smem) != cudaSuccess ||
       ctx->blocks_per_sm < 1)
     return bail(SPH_E_CUDA);
   ctx->coop_grid = ctx->blocks_per_sm * ctx->sm_count;
-  if (cudaMalloc(&ctx->partials, sizeof(sph::Partial) * ctx->coop_grid) != cudaSuccess) return bail(SPH_E_NOMEM);
   *out = ctx;
   return SPH_OK;
 }
@@ -657,6 +760,7 @@ void sph_destroy(SphCtx* ctx) {
                   ctx->sort_src, ctx->sort_orig, ctx->cell_count, ctx->cell_start, ctx->scan_part, ctx->nbr_ff,
                   ctx->cnt_ff, ctx->nbr_fb, ctx->cnt_fb, ctx->rho, ctx->bvec, ctx->dii_aii, ctx->vadv, ctx->P4,
                   ctx->s4, ctx->p_a, ctx->p_b, ctx->Ap, ctx->pmlp, ctx->feat, ctx->mlp, ctx->stage, ctx->partials, ctx->st, ctx->acc, ctx->ring,
+                  ctx->d_scenes, ctx->d_chunks, ctx->d_chunk_scene,
                   ctx->last};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -676,12 +780,11 @@ int sph_set_tables(SphCtx* ctx, const float* w, int32_t nw, const float* g, int3
   int rc = upload_tables(ctx);
   if (rc) return rc;
   int b = 0;
-  CK(sph::jacobi_config(256, ctx->c.sg, &b, &ctx->jac_smem));
+  CK(sph::jacobi_config(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll, ctx->c.sg, &b, &ctx->jac_smem));
   if (b < 1) return fail(ctx, SPH_E_CUDA, "jacobi kernel does not fit");
   if (b != ctx->blocks_per_sm) {
     ctx->blocks_per_sm = b;
     ctx->coop_grid = b * ctx->sm_count;
-    CK(dalloc(ctx->partials, ctx->coop_grid));
   }
   if (ctx->nb) return sort_boundary(ctx);  // psi depends on W
   return SPH_OK;
@@ -691,6 +794,9 @@ int sph_set_boundary(SphCtx* ctx, const float* xb3, const float* vb3, int64_t nb
   if (!ctx || nb < 0 || (nb > 0 && !xb3)) return fail(ctx, SPH_E_INVALID, "bad boundary arguments");
   if (nb > INT32_MAX / 2) return fail(ctx, SPH_E_INVALID, "too many boundary particles");
   CK(cudaSetDevice(ctx->dev));
+  if (ctx->S == 1) ctx->b_off = {0, nb};
+  else if (nb != ctx->b_off[ctx->S])
+    return fail(ctx, SPH_E_INVALID, "a batch takes all scenes' boundary particles, concatenated in scene order");
   ctx->nb = nb;
   ctx->bx_host.assign(xb3, xb3 + 3 * nb);
   ctx->bv_host.assign(3 * nb, 0.f);
@@ -721,6 +827,12 @@ int sph_set_fluid(SphCtx* ctx, const float* x3, const float* v3, int64_t n) {
   if (!ctx || n < 0 || (n > 0 && !x3)) return fail(ctx, SPH_E_INVALID, "bad fluid arguments");
   if (n > INT32_MAX / 64) return fail(ctx, SPH_E_INVALID, "too many fluid particles");
   CK(cudaSetDevice(ctx->dev));
+  if (ctx->S == 1) {
+    if (ctx->f_off[1] != n) ctx->grid_valid = false;
+    ctx->f_off = {0, n};
+  } else if (n != ctx->f_off[ctx->S]) {
+    return fail(ctx, SPH_E_INVALID, "a batch takes all scenes' fluid particles, concatenated in scene order");
+  }
   int rc = alloc_fluid(ctx, n);
   if (rc) return rc;
   const bool resized = (n != ctx->n);
@@ -1004,6 +1116,86 @@ int sph_get_neighbors(SphCtx* ctx, int64_t* ff_off, int32_t* ff_idx, int64_t ff_
   return SPH_OK;
 }
 
+int sph_create_batch(const SphParams* params, const SphSceneDesc* scenes, int32_t nscenes, SphCtx** out) {
+  if (!params || !scenes || !out || nscenes < 1 || nscenes > sph::kMaxScenes) return SPH_E_INVALID;
+  int64_t nf = 0, nbt = 0;
+  for (int sc = 0; sc < nscenes; ++sc) {
+    if (scenes[sc].n < 0 || scenes[sc].nb < 0 || (scenes[sc].n && !scenes[sc].x3) || (scenes[sc].nb && !scenes[sc].xb3))
+      return SPH_E_INVALID;
+    nf += scenes[sc].n;
+    nbt += scenes[sc].nb;
+  }
+  if (nf > INT32_MAX / 64 || nbt > INT32_MAX / 2) return SPH_E_INVALID;
+  int rc = sph_create(params, out);
+  if (rc) return rc;
+  SphCtx* ctx = *out;
+  ctx->S = nscenes;
+  ctx->f_off.assign(nscenes + 1, 0);
+  ctx->b_off.assign(nscenes + 1, 0);
+  ctx->domains.assign(6 * size_t(nscenes), 0.0);
+  for (int sc = 0; sc < nscenes; ++sc) {
+    ctx->f_off[sc + 1] = ctx->f_off[sc] + scenes[sc].n;
+    ctx->b_off[sc + 1] = ctx->b_off[sc] + scenes[sc].nb;
+    for (int a = 0; a < 3; ++a) {
+      ctx->domains[6 * size_t(sc) + a] = scenes[sc].domain_min[a];
+      ctx->domains[6 * size_t(sc) + 3 + a] = scenes[sc].domain_max[a];
+    }
+  }
+  std::vector<float> x(3 * size_t(nf)), v(3 * size_t(nf), 0.f), xb(3 * size_t(nbt)), vb(3 * size_t(nbt), 0.f);
+  bool any_vb = false;
+  for (int sc = 0; sc < nscenes; ++sc) {
+    const SphSceneDesc& d = scenes[sc];
+    std::copy(d.x3, d.x3 + 3 * d.n, x.begin() + 3 * ctx->f_off[sc]);
+    if (d.v3) std::copy(d.v3, d.v3 + 3 * d.n, v.begin() + 3 * ctx->f_off[sc]);
+    if (d.nb) std::copy(d.xb3, d.xb3 + 3 * d.nb, xb.begin() + 3 * ctx->b_off[sc]);
+    if (d.vb3) {
+      std::copy(d.vb3, d.vb3 + 3 * d.nb, vb.begin() + 3 * ctx->b_off[sc]);
+      any_vb = true;
+    }
+  }
+  rc = sph_set_boundary(ctx, xb.data(), any_vb ? vb.data() : nullptr, nbt);
+  if (!rc) rc = sph_set_fluid(ctx, x.data(), v.data(), nf);
+  if (rc) {
+    sph_destroy(ctx);
+    *out = nullptr;
+  }
+  return rc;
+}
+
+int32_t sph_num_scenes(const SphCtx* ctx) { return ctx ? ctx->S : -1; }
+
+int sph_get_scene_ranges(SphCtx* ctx, int64_t* fluid_off, int64_t* boundary_off) {
+  if (!ctx) return SPH_E_INVALID;
+  for (int sc = 0; sc <= ctx->S; ++sc) {
+    if (fluid_off) fluid_off[sc] = ctx->f_off[sc];
+    if (boundary_off) boundary_off[sc] = ctx->b_off[sc];
+  }
+  return SPH_OK;
+}
+
+int sph_get_scene_stats(SphCtx* ctx, int32_t* iterations, double* avg_err, double* v_max, double* dt,
+                        double* sim_time) {
+  if (!ctx) return SPH_E_INVALID;
+  CK(cudaSetDevice(ctx->dev));
+  CK(cudaStreamSynchronize(ctx->stream));
+  StepAcc acc{};
+  DevState st{};
+  CK(cudaMemcpy(&acc, ctx->acc, sizeof(acc), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&st, ctx->st, sizeof(st), cudaMemcpyDeviceToHost));
+  for (int sc = 0; sc < ctx->S; ++sc) {
+    if (iterations) iterations[sc] = acc.iterations[sc];
+    if (avg_err) avg_err[sc] = acc.avg_err[sc];
+    if (v_max) {
+      float f;
+      std::memcpy(&f, &acc.vmax_bits[sc], sizeof(f));
+      v_max[sc] = f;
+    }
+    if (dt) dt[sc] = st.dt64[sc];
+    if (sim_time) sim_time[sc] = st.sim_time[sc];
+  }
+  return SPH_OK;
+}
+
 int sph_set_mlp(SphCtx* ctx, const float* blob, int32_t n) {
   if (!ctx || !blob || n != SPH_MLP_BLOB) return fail(ctx, SPH_E_INVALID, "the network blob has SPH_MLP_BLOB floats");
   for (int c = 0; c < sph::kFeatures; ++c)
@@ -1070,10 +1262,12 @@ int sph_set_dt(SphCtx* ctx, double dt, double inv_dt) {
   CK(cudaStreamSynchronize(ctx->stream));
   DevState s{};
   CK(cudaMemcpy(&s, ctx->st, sizeof(s), cudaMemcpyDeviceToHost));
-  s.dt64 = dt;
-  s.inv_dt64 = inv_dt;
-  s.dt = float(dt);
-  s.inv_dt = float(inv_dt);
+  for (int sc = 0; sc < ctx->S; ++sc) {
+    s.dt64[sc] = dt;
+    s.inv_dt64[sc] = inv_dt;
+    s.dt[sc] = float(dt);
+    s.inv_dt[sc] = float(inv_dt);
+  }
   CK(cudaMemcpy(ctx->st, &s, sizeof(s), cudaMemcpyHostToDevice));
   return SPH_OK;
 }

@@ -54,24 +54,78 @@ struct Consts {
   int max_ff, max_fb, keep_fb;
 };
 
-// Scalars carried across steps (device resident so the step needs no host sync).
+// Independent scenes solved together (batching).  Scene s owns fluid slots
+// [fluid_off[s], fluid_off[s+1]), boundary slots [bound_off[s], ...), its own
+// grid, and global cell ids [cell_base[s], cell_base[s+1]): keys of different
+// scenes never mix, so the cell sort keeps every scene in its slot range and
+// neighbour searches never cross scenes.  Jacobi work is cut into chunks of at
+// most one solve block's worth of particles that never straddle scenes: chunks [chunk_off[s],
+// chunk_off[s+1]) belong to scene s.  A single scene is the case nscenes = 1.
+// A chunk is (threads per block) x (particles per thread) of the solve kernel.
+constexpr int kMaxScenes = 256;
+
+struct SceneTable {
+  int nscenes;
+  int cell_base[kMaxScenes + 1];
+  int fluid_off[kMaxScenes + 1];
+  int bound_off[kMaxScenes + 1];
+  int chunk_off[kMaxScenes + 1];
+  Grid grid[kMaxScenes];
+};
+
+__device__ __forceinline__ int find_scene(const int* __restrict__ off, int nscenes, int i) {
+  int lo = 0, hi = nscenes;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(off + mid) <= i) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Grid and cell-id base of slot i of a fluid (or boundary) array; without a
+// scene table the single grid passed by value applies.
+struct CellFrame {
+  Grid g;
+  int base;
+  int scene;
+};
+__device__ __forceinline__ CellFrame frame_of(const SceneTable* T, const Grid& g0, bool boundary, int i) {
+  CellFrame f;
+  if (!T) {
+    f.g = g0;
+    f.base = 0;
+    f.scene = 0;
+    return f;
+  }
+  const int S = T->nscenes;
+  f.scene = (S == 1) ? 0 : find_scene(boundary ? T->bound_off : T->fluid_off, S, i);
+  f.g = T->grid[f.scene];
+  f.base = T->cell_base[f.scene];
+  return f;
+}
+
+// Scalars carried across steps, per scene (device resident: no host sync per step).
 struct DevState {
-  double dt64, inv_dt64;  // dt, 1/dt with the precision the reference holds them in
-  float dt, inv_dt;       // what the kernels use (float32 kernel arguments)
-  double sim_time;
+  double dt64[kMaxScenes], inv_dt64[kMaxScenes];  // dt, 1/dt as the reference holds them
+  double sim_time[kMaxScenes];
+  float dt[kMaxScenes], inv_dt[kMaxScenes];       // what the kernels use (float32 arguments)
   long long step_index;
 };
 
 // Per-step accumulators, zeroed at the start of every step.
 struct StepAcc {
-  int iterations;
   int flags;
-  double avg_err;
-  unsigned int vmax_bits;
   int max_ff, max_fb;
+  unsigned int bar_count, bar_gen, done_blocks;
+  int all_done;
   int pad0;
   unsigned long long pairs_ff, pairs_fb;
-  unsigned int bar_count, bar_gen, done_blocks, pad1;
+  int iterations[kMaxScenes];
+  int done[kMaxScenes];       // 0 running, 1 converged, 2 stopped at the iteration cap
+  int final_buf[kMaxScenes];  // which pressure buffer holds the scene's final p
+  unsigned int vmax_bits[kMaxScenes];
+  double avg_err[kMaxScenes];
 };
 
 struct Partial {
@@ -205,7 +259,9 @@ __device__ inline bool grid_barrier(StepAcc* acc, unsigned int nblocks, long lon
 
 struct SortArgs {
   int n;
-  Grid grid;
+  Grid grid;                 // used when scenes == nullptr
+  const SceneTable* scenes;  // per-scene grids (nullable)
+  int boundary;              // 1: slots are boundary particles
   const float4* pos;   // unsorted (current state order)
   const int* orig;     // original id per particle of that order
   int* key;
@@ -220,6 +276,7 @@ struct SortArgs {
 struct BuildArgs {
   int n, nb;
   Grid grid;
+  const SceneTable* scenes;
   Consts c;
   const float* w_table;
   const float* g_table;
@@ -248,6 +305,10 @@ struct BuildArgs {
 
 struct JacobiArgs {
   int n;
+  int nscenes, nchunks;
+  const int2* chunks;        // [start, end) particle slots of each chunk
+  const int* chunk_scene;
+  const SceneTable* scenes;
   Consts c;
   const float* g_table;
   const float4* pos;
@@ -263,7 +324,7 @@ struct JacobiArgs {
   float4* P4;
   float4* s4;              // (s, A1)
   float* Ap;
-  Partial* partials;       // one per block
+  Partial* partials;       // one per chunk
   DevState* st;
   StepAcc* acc;
   SphStepStats* ring;      // per-step stats ring buffer
@@ -281,6 +342,7 @@ struct JacobiArgs {
 struct PsiArgs {
   int nb;
   Grid grid;
+  const SceneTable* scenes;
   Consts c;
   const float* w_table;
   float4* bpos;            // in: x,y,z; out: w = psi
@@ -295,8 +357,10 @@ cudaError_t launch_psi_sorted(const PsiArgs& a, float* psi_sorted, int block, cu
 cudaError_t launch_gather(int n, const int* sort_src, const int* sort_orig, const float4* pos_in,
                           const float4* vel_in, const float* p_in, float4* pos_out, float4* vel_out,
                           int* orig_out, float* p_out, cudaStream_t s);
-cudaError_t jacobi_config(int block, int sg, int* blocks_per_sm, size_t* smem);
-cudaError_t launch_jacobi(const JacobiArgs& a, int grid, int block, size_t smem, cudaStream_t s);
+bool jacobi_variant_ok(int block, int ppt, int unroll);
+cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, int* blocks_per_sm, size_t* smem);
+cudaError_t launch_jacobi(const JacobiArgs& a, int grid, int block, int ppt, int unroll, size_t smem,
+                          cudaStream_t s);
 cudaError_t launch_pack_fluid(int n, const float* x3, const float* v3, float4* pos, float4* vel, int* orig,
                               float* p, cudaStream_t s);
 cudaError_t launch_unsort4(int n, const int* orig, const float4* src, int component, float* out, cudaStream_t s);

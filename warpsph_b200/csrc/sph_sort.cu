@@ -28,8 +28,9 @@ __global__ void k_cell_keys(SortArgs a) {
   bool live = i < a.n;
   int key = -1;
   if (live) {
-    float4 x = a.pos[i];
-    key = cell_index(a.grid, cell_coord(a.grid, x.x, x.y, x.z));
+    const float4 x = a.pos[i];
+    const CellFrame f = frame_of(a.scenes, a.grid, a.boundary != 0, i);
+    key = f.base + cell_index(f.g, cell_coord(f.g, x.x, x.y, x.z));
     a.key[i] = key;
   }
   unsigned int active = __ballot_sync(0xffffffffu, live);

@@ -38,8 +38,11 @@ class SolverParams:
     keep_fb_lists: bool = False
     use_graph: bool = True
     device: int = 0
-    block_size: int = 0
+    block_size: int = 0           # neighbour build threads per block (0 = 128)
     timeout_ms: int = 2000
+    jacobi_block: int = 0         # pressure solve threads per block (0 = 256)
+    jacobi_ppt: int = 0           # particles per solve thread (0 = 1)
+    jacobi_unroll: int = 0        # solve neighbour-loop unroll (0 = 4)
     dt0: float | None = None      # None: TIME_STEP_MAX (IISPH.py:747)
     domain_min: tuple = (0.0, 0.0, 0.0)
     domain_max: tuple = (0.0, 0.0, 0.0)
@@ -104,6 +107,9 @@ class SolverParams:
         p.device = self.device
         p.block_size = self.block_size
         p.timeout_ms = self.timeout_ms
+        p.jacobi_block = self.jacobi_block
+        p.jacobi_ppt = self.jacobi_ppt
+        p.jacobi_unroll = self.jacobi_unroll
         return p
 
     @classmethod
