@@ -35,7 +35,13 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "IISPH steps/s at 1M particles, 0.1% density err; learned warm-start vs plain"
 PRESET = "dam_break_1m"
-KERNELS_PER_STEP = 8  # cell_keys, scan_part, scan_final, scatter, cell_sort, gather, build, jacobi
+# cell_keys, scan_part, scan_final, scatter, cell_sort, gather, build, jacobi
+# (+ mlp_infer with the learned warm start)
+KERNELS_PER_STEP = 8
+
+
+def kernels_per_step(warm: str) -> int:
+    return KERNELS_PER_STEP + (1 if warm == "mlp" else 0)
 
 
 def _peaks():
@@ -220,7 +226,10 @@ def bench_ours(args):
         s = fresh(headline)
         _lib.check(s._ctx, s._lib.sph_launch_steps(s._ctx, K))
         torch.cuda.synchronize()
-        print(json.dumps({"profile_run": True, "steps": K, "stats": s.stats_history(K)[-1]}))
+        hist = s.stats_history(K)
+        print(json.dumps({"profile_run": True, "steps": K, "n": n,
+                          "iterations": [h["iterations"] for h in hist],
+                          "n_ff_pairs": [h["n_ff_pairs"] for h in hist]}))
         s.close()
         return
 
@@ -257,28 +266,36 @@ def bench_ours(args):
     # dominant kernel: per-launch CUDA-event time of the persistent solve over the same K steps
     s = fresh(headline)
     st = stream_of(s)
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(K)]
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(6)] for _ in range(K)]
     torch.cuda.synchronize()
     for e in ev:
         e[0].record(st)
-        _lib.check(s._ctx, s._lib.sph_launch_phase(s._ctx, 0))
+        _lib.check(s._ctx, s._lib.sph_launch_phase(s._ctx, 0))  # sort + neighbour build
         e[1].record(st)
+        _lib.check(s._ctx, s._lib.sph_launch_phase(s._ctx, 2))  # warm-start inference
         e[2].record(st)
-        _lib.check(s._ctx, s._lib.sph_launch_phase(s._ctx, 1))
         e[3].record(st)
+        _lib.check(s._ctx, s._lib.sph_launch_phase(s._ctx, 3))  # k_jacobi alone
+        e[4].record(st)
     torch.cuda.synchronize()
     hk = s.stats_history(K)
     check_flags(hk)
     s.close()
     t_front = [e[0].elapsed_time(e[1]) for e in ev]
-    t_jac = [e[2].elapsed_time(e[3]) for e in ev]
+    t_warm = [e[1].elapsed_time(e[2]) for e in ev]
+    t_jac = [e[3].elapsed_time(e[4]) for e in ev]
     bytes_launch = [h["iterations"] * (100.0 * n + 8.0 * h["n_ff_pairs"]) + 112.0 * n for h in hk]
     achieved = sum(bytes_launch) / (sum(t_jac) / 1000.0) / 1e9
     peak, peak_kind = _peaks()
+    # DRAM traffic per launch: the ncu-measured ratio of dram bytes to these
+    # algorithmic bytes on a captured k_jacobi launch, applied to this run's
+    # mean launch (traffic grows with iterations x pairs like the bytes rule)
     traffic = None
     tf = ROOT / "profiles" / "jacobi_traffic.json"
     if tf.exists():
-        traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+        ratio = json.loads(tf.read_text()).get("traffic_over_algorithmic")
+        if ratio:
+            traffic = ratio * sum(bytes_launch) / len(bytes_launch)
 
     # end to end through the C ABI with host buffers: every step uploads its
     # input state (x, v) from pinned memory and reads back x, v, p
@@ -323,7 +340,8 @@ def bench_ours(args):
             "particle_updates_per_s": value * n,
             "jacobi_iterations_mean": float(np.mean(iters)), "avg_err_max": float(np.max([h["avg_err"] for h in hist])),
             "n_ff_pairs_mean": float(np.mean([h["n_ff_pairs"] for h in hist])),
-            "phase_ms_mean": {"front": float(np.mean(t_front)), "solve": float(np.mean(t_jac))},
+            "phase_ms_mean": {"front": float(np.mean(t_front)), "warm_start": float(np.mean(t_warm)),
+                              "jacobi": float(np.mean(t_jac))},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "k_jacobi (persistent solve + kick/drift)",
@@ -331,7 +349,7 @@ def bench_ours(args):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": 28 * n + 80},
-            "gpu_launches": KERNELS_PER_STEP * K,
+            "gpu_launches": kernels_per_step(headline) * K,
             "clocks": clock,
         }
         print(json.dumps(line), flush=True)

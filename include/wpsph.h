@@ -159,14 +159,18 @@ int sph_step(SphCtx* ctx, SphStepStats* out);
 int sph_steps(SphCtx* ctx, int32_t nsteps, SphStepStats* last);
 int sph_get_stats_history(SphCtx* ctx, SphStepStats* out, int32_t count);
 
-/* Asynchronous forms for callers that time with CUDA events on sph_stream():
- * enqueue nsteps steps, or one phase of a step (0 = cell sort + neighbour
- * build + advection prediction, 1 = pressure solve + kick/drift/CFL), with no
- * host synchronisation.  Flags surface at the next sph_get_stats/sph_step. */
+/* Asynchronous form for callers that time with CUDA events on sph_stream():
+ * enqueue nsteps steps with no host synchronisation.  Flags surface at the
+ * next sph_get_stats/sph_step. */
 int sph_launch_steps(SphCtx* ctx, int32_t nsteps);
 /* Capture the step's CUDA graph now (it is otherwise captured by the first
  * step), so that a caller's first timed step excludes the capture. */
 int sph_prepare(SphCtx* ctx);
+/* Enqueue one part of a step without the graph (for per-kernel timing on
+ * sph_stream): 0 = cell sort + neighbour build, 1 = pressure solve (2 then 3),
+ * 2 = warm-start inference only (a no-op unless SPH_WARM_MLP),
+ * 3 = persistent Jacobi solve with the fused kick/drift/CFL only.
+ * Phases 0, 1 (or 0, 2, 3) in order make one step. */
 int sph_launch_phase(SphCtx* ctx, int32_t phase);
 
 /* IISPH.neighbor_search() (IISPH.py:1408-1482): cell sort + neighbour build +

@@ -501,7 +501,8 @@ int enqueue_front(SphCtx* ctx) {
   return SPH_OK;
 }
 
-int enqueue_solve(SphCtx* ctx) {
+// learned warm start: the network's prediction becomes the first iterate
+int enqueue_warm(SphCtx* ctx) {
   if (ctx->P.warm_start == SPH_WARM_MLP) {
     sph::MlpInferArgs m{};
     m.n = ctx->n;
@@ -514,6 +515,11 @@ int enqueue_solve(SphCtx* ctx) {
     m.P4 = ctx->P4;
     CK(sph::launch_mlp_infer(m, ctx->sm_count, ctx->stream));
   }
+  return SPH_OK;
+}
+
+// the persistent pressure solve with the fused kick, drift and CFL update
+int enqueue_jacobi(SphCtx* ctx) {
   sph::JacobiArgs j{};
   j.n = int(ctx->n);
   j.nscenes = ctx->S;
@@ -557,6 +563,12 @@ int enqueue_solve(SphCtx* ctx) {
   CK(sph::launch_jacobi(j, ctx->coop_grid, ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll, ctx->jac_smem,
                         ctx->stream));
   return SPH_OK;
+}
+
+int enqueue_solve(SphCtx* ctx) {
+  int rc = enqueue_warm(ctx);
+  if (rc) return rc;
+  return enqueue_jacobi(ctx);
 }
 
 int enqueue_step(SphCtx* ctx) {
@@ -941,11 +953,16 @@ int sph_prepare(SphCtx* ctx) {
 }
 
 int sph_launch_phase(SphCtx* ctx, int32_t phase) {
-  if (!ctx || phase < 0 || phase > 1) return fail(ctx, SPH_E_INVALID, "phase must be 0 or 1");
+  if (!ctx || phase < 0 || phase > 3) return fail(ctx, SPH_E_INVALID, "phase must be 0, 1, 2 or 3");
   CK(cudaSetDevice(ctx->dev));
   int rc = ensure_ready(ctx);
   if (rc) return rc;
-  return phase == 0 ? enqueue_front(ctx) : enqueue_solve(ctx);
+  switch (phase) {
+    case 0: return enqueue_front(ctx);
+    case 1: return enqueue_solve(ctx);
+    case 2: return enqueue_warm(ctx);
+    default: return enqueue_jacobi(ctx);
+  }
 }
 
 int sph_get_stats_history(SphCtx* ctx, SphStepStats* out, int32_t count) {
