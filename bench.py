@@ -195,15 +195,22 @@ def bench_ours(args):
     def stream_of(s):
         return torch.cuda.ExternalStream(s._lib.sph_stream(s._ctx), device=dev)
 
-    def check_flags(hist):
+    # a dam break under gravity cannot outrun free fall from the box height:
+    # a step faster than 10x that is a diverged run, not a measurement
+    v_limit = 10.0 * (2.0 * 9.81 * scene.box[1]) ** 0.5
+
+    def check_flags(hist, headline_run=True):
         flags = 0
         for h in hist:
             flags |= h["flags"]
         bad = _lib.SPH_F_TIMEOUT | _lib.SPH_F_NONFINITE | _lib.SPH_F_FF_OVERFLOW | _lib.SPH_F_FB_OVERFLOW
         if flags & bad:
             raise RuntimeError(f"step flags {flags:#x} in a timed region")
+        vmax = max(h["v_max"] for h in hist)
+        if headline_run and vmax > v_limit:
+            raise RuntimeError(f"v_max {vmax:.3g} m/s exceeds {v_limit:.3g} m/s: the run diverged")
 
-    def timed_steps(s, count):
+    def timed_steps(s, count, headline_run=True):
         st = stream_of(s)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -212,7 +219,7 @@ def bench_ours(args):
         e1.record(st)
         e1.synchronize()
         hist = s.stats_history(count)
-        check_flags(hist)
+        check_flags(hist, headline_run)
         return e0.elapsed_time(e1), hist
 
     # warm-up: W steps on a throwaway solver (clocks, module load, graph capture)
@@ -255,13 +262,15 @@ def bench_ours(args):
     modes = {}
     for mode in ("zero", "half", "mlp"):
         if mode == headline:
-            modes[mode] = {"steps_per_s": K / (ms / 1000.0), "jacobi_iterations": int(sum(iters))}
+            modes[mode] = {"steps_per_s": K / (ms / 1000.0), "jacobi_iterations": int(sum(iters)),
+                           "v_max_max": float(max(h["v_max"] for h in hist))}
             continue
         s = fresh(mode)
-        m_ms, m_hist = timed_steps(s, K)
+        m_ms, m_hist = timed_steps(s, K, headline_run=False)
         s.close()
         modes[mode] = {"steps_per_s": K / (m_ms / 1000.0),
-                       "jacobi_iterations": int(sum(h["iterations"] for h in m_hist))}
+                       "jacobi_iterations": int(sum(h["iterations"] for h in m_hist)),
+                       "v_max_max": float(max(h["v_max"] for h in m_hist))}
 
     # dominant kernel: per-launch CUDA-event time of the persistent solve over the same K steps
     s = fresh(headline)
@@ -339,6 +348,7 @@ def bench_ours(args):
             "speedup_vs_plain": value / (world * modes["zero"]["steps_per_s"]) if modes.get("zero") else None,
             "particle_updates_per_s": value * n,
             "jacobi_iterations_mean": float(np.mean(iters)), "avg_err_max": float(np.max([h["avg_err"] for h in hist])),
+            "v_max_max": float(np.max([h["v_max"] for h in hist])),
             "n_ff_pairs_mean": float(np.mean([h["n_ff_pairs"] for h in hist])),
             "phase_ms_mean": {"front": float(np.mean(t_front)), "warm_start": float(np.mean(t_warm)),
                               "jacobi": float(np.mean(t_jac))},

@@ -77,7 +77,7 @@ typedef struct SphParams {
   int32_t timeout_ms;    /* bound on every grid-wide wait */
   int32_t jacobi_block;  /* threads per block of the pressure solve: 128 or 256 (0 = 256) */
   int32_t jacobi_ppt;    /* particles per solve thread: 1 or 2 (0 = 1) */
-  int32_t jacobi_unroll; /* neighbour-loop unroll of the solve: 2, 4 or 8 (0 = 4) */
+  int32_t jacobi_unroll; /* neighbour-loop unroll of the solve: 2, 4 or 8 (0 = 2) */
   int32_t reserved[2];
 } SphParams;
 
@@ -226,15 +226,24 @@ int sph_boundary_psi_noalloc(const SphParams* params, const float* d_xb3, int64_
  * computes and uses it as the solve's first iterate; the unchanged Jacobi
  * loop (at least 2 iterations, average density error <= eta) still decides
  * convergence.
+ * The network is residual on the previous step's pressure: with input 3,
+ * u = asinh(p_prev / (rho0 g h)), taken in FP32 (no BF16 rounding on the
+ * skip path), the prediction is
+ *   p = sinh(max(u + min(y * t_scale, SPH_MLP_MAX_RISE), 0)) * rho0 * g * h;
+ * the bounded rise keeps one over-predicted particle (which the solve's test,
+ * counting only compressed particles, would not see) from being kicked out.
  * Weights travel as one FP32 blob of SPH_MLP_BLOB floats:
  *   mu[10], sd[10]   input standardisation (x - mu) / sd
- *   t_scale          output unit: p = sinh(max(y * t_scale, 0)) * rho0 * g * h
+ *   t_scale          output unit of y
  *   W1[10][64] b1[64] W2[64][64] b2[64] w3[64] b3   (SPH_MLP_PARAMS, W[in][out])
- * Training targets are t = asinh(p / (rho0 g h)) of the converged pressure
- * (pressures span orders of magnitude; asinh keeps them on one scale). */
+ * sph_get_features gives t = asinh(p / (rho0 g h)) of the converged pressure
+ * (pressures span orders of magnitude; asinh keeps them on one scale); the
+ * network is trained on the residual t - u.  sph_mlp_train and sph_mlp_eval
+ * regress y * t_scale on whatever target array they are given. */
 #define SPH_MLP_FEATURES 10
 #define SPH_MLP_PARAMS 4929
 #define SPH_MLP_BLOB 4950
+#define SPH_MLP_MAX_RISE 0.5f
 
 typedef struct SphMlpTrainConfig {
   int32_t epochs;

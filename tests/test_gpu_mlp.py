@@ -39,12 +39,17 @@ def test_training_reduces_loss():
     from warpsph_b200 import learned
 
     f, t = _data(n=60000, seed=1)
-    blob0 = learned.init_blob(f, t, seed=0)
-    l0 = M.loss_and_grad(blob0, f[:4096], t[:4096])[0]
+    r = learned.residual_target(f, t)  # what the network regresses: t - input 3
+    blob0 = learned.init_blob(f, r, seed=0)
+    l0 = M.loss_and_grad(blob0, f[:4096], r[:4096])[0]
     blob, losses = learned.train(f, t, epochs=8, batch=2048, lr=1e-3, seed=0, blob=blob0)
     assert losses[-1] < 0.2 * losses[0]
-    l1 = M.loss_and_grad(blob, f[:4096], t[:4096])[0]
+    l1 = M.loss_and_grad(blob, f[:4096], r[:4096])[0]
     assert l1 < 0.2 * l0
+    # the prediction adds the skip input back
+    y = learned.evaluate(blob, f[:64])
+    want = f[:64, 3] + np.minimum(y * blob[20], 0.5)
+    assert np.allclose(learned.predict(blob, f[:64]), want, rtol=0, atol=1e-6)
 
 
 def test_learned_warm_start_reduces_iterations():

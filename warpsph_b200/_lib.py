@@ -71,6 +71,7 @@ class SphMlpTrainConfig(ctypes.Structure):
 SPH_MLP_FEATURES = 10
 SPH_MLP_PARAMS = 4929
 SPH_MLP_BLOB = 4950
+SPH_MLP_MAX_RISE = 0.5
 
 
 class SphSceneDesc(ctypes.Structure):

@@ -71,7 +71,7 @@ def autotune(scenes, params, warm=10, steps=20, use_cache=True, verbose=False) -
             print("build", bb, t)
         if t < best_t:
             best_build, best_t = bb, t
-    best = (256, 1, 4)
+    best = (256, 1, 2)
     for blk, ppt, unr in SOLVE_SHAPES:
         t = _time(scenes, params.replace(block_size=best_build, jacobi_block=blk, jacobi_ppt=ppt,
                                          jacobi_unroll=unr), warm, steps)

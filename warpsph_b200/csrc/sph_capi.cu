@@ -750,7 +750,7 @@ int sph_create(const SphParams* params, SphCtx** out) {
   if (cudaMemcpy(ctx->st, &s, sizeof(s), cudaMemcpyHostToDevice) != cudaSuccess) return bail(SPH_E_CUDA);
   ctx->jac_block = P.jacobi_block ? P.jacobi_block : 256;
   ctx->jac_ppt = P.jacobi_ppt ? P.jacobi_ppt : 1;
-  ctx->jac_unroll = P.jacobi_unroll ? P.jacobi_unroll : 4;
+  ctx->jac_unroll = P.jacobi_unroll ? P.jacobi_unroll : 2;
   if (!sph::jacobi_variant_ok(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll)) return bail(SPH_E_INVALID);
   ctx->chunk = ctx->jac_block * ctx->jac_ppt;
   if (sph::jacobi_config(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll, ctx->c.sg, &ctx->blocks_per_sm,

@@ -144,9 +144,17 @@ __device__ __forceinline__ void feature_frag(const MlpSmem& s, const float* __re
 
 // ------------------------------------------------------------------ inference
 
-// The predicted pressure sinh(max(y t_scale, 0)) rho0 g h of every particle,
-// written as the solve's first iterate p_1 together with P4 = (d_ii p_1,
-// p_1 / rho^2) for the first Jacobi pass.
+// The predicted pressure of every particle, written as the solve's first
+// iterate p_1 together with P4 = (d_ii p_1, p_1 / rho^2) for the first Jacobi
+// pass.  The network is residual on the previous step's pressure: with
+// u = asinh(p_prev / (rho0 g h)) (input 3, read here in float32, so the skip
+// path carries no bf16 rounding) the prediction is
+//   p_1 = sinh(max(u + min(y t_scale, kMaxRise), 0)) rho0 g h.
+// The rise over the previous pressure is bounded: the solve's stopping test
+// only counts compressed particles, so an over-predicted pressure (a network
+// extrapolating on an outlier such as a splash particle with a tiny a_ii) could
+// pass it after the minimum 2 iterations and kick the particle out of the
+// fluid.  Lower predictions only move the start toward p = 0.
 __global__ void __launch_bounds__(128) k_mlp_infer(MlpInferArgs a) {
   __shared__ MlpSmem s;
   load_weights(s, a.w);
@@ -166,8 +174,8 @@ __global__ void __launch_bounds__(128) k_mlp_infer(MlpInferArgs a) {
         const long long i = r0 + g + 8 * h;
         if (i < a.n) {
           if (a.p0) {
-            // the target is asinh(p / (rho0 g h)) in units of t_scale
-            const float p = sinhf(fmaxf(f.y[2 * h] * s.t_scale, 0.f)) * a.p_unit;
+            const float u = __ldg(a.feat + i * kFeatures + 3);
+            const float p = sinhf(fmaxf(u + fminf(f.y[2 * h] * s.t_scale, kMaxRise), 0.f)) * a.p_unit;
             const float4 da = __ldg(a.dii_aii + i);
             const float rho = __ldg(a.rho + i);
             a.p0[i] = p;

@@ -9,6 +9,9 @@
 namespace sph {
 
 constexpr int kH = 64;        // hidden width
+// largest rise of asinh(p / (rho0 g h)) over the previous step's value that
+// the warm start may predict
+constexpr float kMaxRise = SPH_MLP_MAX_RISE;
 constexpr int kIn = 16;       // kFeatures padded to one k-tile
 constexpr int kW1Pitch = 24;  // row pitch (bf16) of w1f: 8 rows hit 8 distinct bank groups
 constexpr int kWPitch = 72;   // row pitch (bf16) of the 64-wide matrices

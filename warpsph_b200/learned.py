@@ -4,7 +4,10 @@ The network (10 -> 64 -> 64 -> 1, BF16 tensor cores) is trained on the
 solver's own converged pressures: every step of a set of dam-break scenes
 exports each particle's 10 inputs and asinh(p / (rho0 g h)) of its converged
 pressure (sph_get_features), a sample of them forms the training set, and
-sph_mlp_train fits the network on the GPU (Adam, MSE).  At run time
+sph_mlp_train fits the network on the GPU (Adam, MSE).  The network is
+residual: it predicts the change of asinh(p / (rho0 g h)) from the previous
+step's value (input 3), which the inference kernel adds back in float32, so
+the network's BF16 arithmetic only touches the small correction.  At run time
 SPH_WARM_MLP starts the relaxed Jacobi solve from the prediction; the solve's
 stopping rule is unchanged.
 
@@ -51,10 +54,19 @@ def init_blob(feat: np.ndarray, target: np.ndarray, seed: int = 0) -> np.ndarray
     return blob
 
 
+SKIP = 3  # input carried around the network: asinh(p_prev / (rho0 g h))
+
+
+def residual_target(feat, target) -> np.ndarray:
+    """What the network regresses: the target minus the skip input."""
+    return (np.asarray(target, np.float32) - np.asarray(feat, np.float32)[:, SKIP]).astype(np.float32)
+
+
 def train(feat, target, epochs=20, batch=4096, lr=1e-3, seed=0, device=0, blob=None):
-    """Fit the network on the GPU; returns (blob, per-epoch loss)."""
+    """Fit the network on the GPU to (feat, target), target = asinh(p / (rho0 g h))
+    of the converged pressure; returns (blob, per-epoch loss)."""
     feat = np.ascontiguousarray(feat, np.float32)
-    target = np.ascontiguousarray(target, np.float32)
+    target = np.ascontiguousarray(residual_target(feat, target), np.float32)
     blob = init_blob(feat, target, seed) if blob is None else np.array(blob, np.float32)
     cfg = _lib.SphMlpTrainConfig(epochs=epochs, batch=batch, lr=lr, beta1=0.9, beta2=0.999, eps=1e-8,
                                  seed=seed, device=device)
@@ -65,8 +77,17 @@ def train(feat, target, epochs=20, batch=4096, lr=1e-3, seed=0, device=0, blob=N
     return blob, losses[:epochs]
 
 
+def predict(blob, feat, device=0) -> np.ndarray:
+    """Predicted asinh(p / (rho0 g h)) before the clamp at 0: the skip input
+    plus the network's correction, whose rise is bounded by SPH_MLP_MAX_RISE."""
+    feat = np.ascontiguousarray(feat, np.float32)
+    y = evaluate(blob, feat, device=device)
+    return feat[:, SKIP] + np.minimum(y * np.float32(blob[2 * NF]), np.float32(_lib.SPH_MLP_MAX_RISE))
+
+
 def evaluate(blob, feat, target=None, device=0):
-    """Network outputs (units of t_scale) and, with target, (loss, gradient)."""
+    """Network outputs (units of t_scale) and, with a target (already residual),
+    (loss, gradient) of the mean squared error."""
     feat = np.ascontiguousarray(feat, np.float32)
     blob = np.ascontiguousarray(blob, np.float32)
     pred = np.zeros(len(feat), np.float32)
@@ -83,9 +104,11 @@ def evaluate(blob, feat, target=None, device=0):
     return pred, float(grad[-1]), grad[:-1]
 
 
-def collect(scenes, steps, per_step, params_for, seed=0, warm="half"):
+def collect(scenes, steps, per_step, params_for, seed=0, warm="half", skip=0):
     """Run each scene for ``steps`` steps, sampling ``per_step`` (input, target)
-    pairs per step.  ``params_for(scene)`` gives the SolverParams."""
+    pairs per step after the first ``skip`` steps (the start-up transient,
+    whose pressure jumps would dominate a mean-squared loss).
+    ``params_for(scene)`` gives the SolverParams."""
     from .solver import IISPH
 
     rng = np.random.default_rng(seed)
@@ -96,8 +119,10 @@ def collect(scenes, steps, per_step, params_for, seed=0, warm="half"):
         n = sc.n
         f = np.zeros((n, NF), np.float32)
         t = np.zeros(n, np.float32)
-        for _ in range(steps):
+        for k in range(steps):
             sol.step()
+            if k < skip:
+                continue
             _lib.check(sol._ctx, sol._lib.sph_get_features(sol._ctx, _lib.ptr(f), _lib.ptr(t)))
             pick = rng.choice(n, size=min(per_step, n), replace=False)
             feats.append(f[pick].copy())

@@ -4,7 +4,8 @@
 
 Data: the solver's own converged pressures on the 64 batched dam-break scenes
 (`scenes.batched_scenes`, 0.01 m spacing, dt 5e-4, 1024-sample tables,
-g = 9.81), `--steps` steps each, sampled evenly to `--pairs` pairs.  Training:
+g = 9.81), `--steps` steps each, sampled evenly to `--pairs` pairs after each
+scene's first `--skip` steps.  Training:
 Adam, lr 1e-3, MSE, on the GPU with libwpsph's own kernels.  Output:
 warpsph_b200/data/warm_start_mlp.npz.
 """
@@ -31,16 +32,17 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--out", default=str(learned.DEFAULT_WEIGHTS))
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--skip", type=int, default=20, help="start-up steps of each scene left out of the data")
     a = ap.parse_args()
     scenes = batched_scenes(count=a.scenes)
-    per_step = max(1, a.pairs // (a.scenes * a.steps))
+    per_step = max(1, a.pairs // (a.scenes * max(1, a.steps - a.skip)))
     t0 = time.time()
     params = SolverParams(diameter=0.01, gravity=9.81, w_table_size=1024, g_table_size=1024)
-    feat, target = learned.collect(scenes, a.steps, per_step, lambda sc: params, seed=a.seed)
+    feat, target = learned.collect(scenes, a.steps, per_step, lambda sc: params, seed=a.seed, skip=a.skip)
     t1 = time.time()
     blob, losses = learned.train(feat, target, epochs=a.epochs, lr=a.lr, seed=a.seed)
     t2 = time.time()
-    meta = dict(pairs=len(target), scenes=a.scenes, steps=a.steps, epochs=a.epochs, lr=a.lr,
+    meta = dict(pairs=len(target), scenes=a.scenes, steps=a.steps, skip=a.skip, epochs=a.epochs, lr=a.lr,
                 losses=losses.tolist(), collect_s=t1 - t0, train_s=t2 - t1)
     learned.save(a.out, blob, meta=json.dumps(meta))
     print(json.dumps(meta))
