@@ -105,10 +105,32 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def run_cpu_reference(budget_s: float, max_steps: int, nthreads: int = 0, state=None):
-    """The reference algorithm (CPU oracle, FP32, OpenMP) on the same scene,
-    from ``state`` = (x, v, dt, step_index) when given (the GPU run's state at
-    the start of its timed region), else from the initial state."""
+# Jacobi iterations of the reference algorithm (p <- 0 start) on the 1M dam
+# break, per step over steps [0, 20) and in total over [20, 500), as counted by
+# the parity-tested solver (iteration counts agree with the oracle to +-1).
+REF_ITERS_FIRST20 = [101, 101, 101, 101, 101, 92, 2, 2, 2, 6, 4, 2, 2, 2, 2, 2, 2, 2, 2, 2]
+REF_ITERS_20_500 = 3154
+
+
+def ref_iterations(K: int) -> float:
+    """Reference-algorithm Jacobi iterations over steps [0, K) of the workload."""
+    if K <= 20:
+        return float(sum(REF_ITERS_FIRST20[:K]))
+    return float(sum(REF_ITERS_FIRST20)) + (K - 20) * REF_ITERS_20_500 / 480.0
+
+
+def run_cpu_reference(budget_s: float, max_steps: int, nthreads: int = 0):
+    """The reference algorithm (CPU oracle, FP32, OpenMP on all host threads)
+    on the same scene.  Two measurements:
+
+    * unit costs at the initial state: one step with 2 and one with 12 fixed
+      Jacobi iterations give the cost of an iteration and of the rest of a step
+      (sort, neighbour search, density and advection terms, kick, drift); the
+      value is the steps/s of steps [0, K) at the reference algorithm's own
+      iteration count for that range (`ref_iterations`);
+    * the first steps from the initial state, timed as they run until the
+      budget is spent (they are the most expensive ones, up to 101 iterations).
+    """
     from oracle import oracle
     from warpsph_b200.params import preset_params
     from warpsph_b200.scenes import preset_scene
@@ -121,38 +143,52 @@ def run_cpu_reference(budget_s: float, max_steps: int, nthreads: int = 0, state=
     tabs = kernel_tables(params)
     nt = nthreads or oracle.max_threads()
     psi = oracle.boundary_psi(op, scene.boundary_x, tables=tabs, nthreads=nt)
-    if state is None:
-        x, v, dt, start = scene.fluid_x.copy(), scene.fluid_v.copy(), params.dt_max, 0
-    else:
-        x, v, dt, start = state
-    inv_dt = 1.0 / dt
-    steps, t_total, iters = 0, 0.0, []
-    while steps < max_steps and (steps == 0 or t_total < budget_s):
+    x0, v0, dt0 = scene.fluid_x.copy(), scene.fluid_v.copy(), params.dt_max
+
+    def one(x, v, dt, fixed=-1):
         t0 = time.perf_counter()
-        r = oracle.step(op, x, v, scene.boundary_x, None, psi, dt, inv_dt, tables=tabs, export=False,
-                        nthreads=nt)
-        t_total += time.perf_counter() - t0
-        x, v, dt, inv_dt = r["x"], r["v"], r["dt_next"], r["inv_dt_next"]
+        r = oracle.step(op, x, v, scene.boundary_x, None, psi, dt, 1.0 / dt, tables=tabs, export=False,
+                        nthreads=nt, fixed_iters=fixed)
+        return time.perf_counter() - t0, r
+
+    t2, _ = one(x0, v0, dt0, fixed=2)
+    t12, _ = one(x0, v0, dt0, fixed=12)
+    t_iter = max((t12 - t2) / 10.0, 1e-9)
+    t_base = max(t2 - 2.0 * t_iter, 0.0)
+    K = max(1, max_steps)
+    iters_ref = ref_iterations(K)
+    value = K / (K * t_base + iters_ref * t_iter)
+
+    x, v, dt = x0, v0, dt0
+    steps, t_total, iters = 0, 0.0, []
+    while steps < K and (steps == 0 or t_total < budget_s):
+        t, r = one(x, v, dt)
+        t_total += t
+        x, v, dt = r["x"], r["v"], r["dt_next"]
         iters.append(r["iterations"])
         steps += 1
-    return {"value": steps / t_total, "unit": "steps/s", "cores": nt, "kind": "port",
-            "sample": f"steps [{start}, {start + steps}) of the 1M-particle dam break "
-                      f"(FP32 oracle, {nt} OpenMP threads); Jacobi iterations {iters}"}
+    return {"value": value, "unit": "steps/s", "cores": nt, "kind": "port",
+            "sample": (f"FP32 oracle, {nt} OpenMP threads, 1M-particle dam break: {t_iter * 1e3:.1f} ms per "
+                       f"Jacobi iteration and {t_base * 1e3:.1f} ms for the rest of a step, measured at the "
+                       f"initial state (steps with 2 and 12 fixed iterations); value = steps/s of steps [0, {K}) "
+                       f"at the reference algorithm's {iters_ref:.0f} iterations for that range"),
+            "ms_per_iteration": t_iter * 1e3, "ms_step_base": t_base * 1e3,
+            "first_steps": {"steps": steps, "steps_per_s": steps / t_total, "iterations": iters}}
 
 
 def bench_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    base = run_cpu_reference(budget_s=150.0, max_steps=max(1, args.steps))
+    base = run_cpu_reference(budget_s=60.0, max_steps=max(1, args.steps))
     line = {
         "impl": "reference", "metric": METRIC, "value": base["value"], "unit": "steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 / base["value"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"dam break, 1,000,000 fluid + 206,464 boundary particles, steps [0, {args.steps}) "
-                               "from the initial state (CPU: the first steps of that range, time-bounded), "
-                               "0.1% avg density err", "preset": PRESET, "warm_start": "zero"},
+                               "from the initial state, 0.1% avg density err (CPU: unit costs sampled at the "
+                               "initial state, see cpu_baseline.sample)", "preset": PRESET, "warm_start": "zero"},
         "cpu_baseline": base,
         "e2e": {"value": base["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -169,18 +205,13 @@ def bench_ours(args):
     from warpsph_b200.scenes import preset_scene
     from warpsph_b200.solver import IISPH
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from warpsph_b200 import ranks
+
+    rank, world, local = ranks.env_rank()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    # N ranks = N independent replicas of the scene; only the timing is reduced
+    dist = ranks.init("nccl", device=dev)
 
     scene = preset_scene(PRESET)
     n = scene.n
@@ -251,10 +282,7 @@ def bench_ours(args):
     ms, hist = timed_steps(sol, K)
     clock = clocks.stop()
     sol.close()
-    ms_t = torch.tensor([ms], device=dev)
-    if dist:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = ranks.max_over_ranks(ms, dist, dev)
     value = world * K / (ms_max / 1000.0)
     iters = [h["iterations"] for h in hist]
 
@@ -325,15 +353,12 @@ def bench_ours(args):
         _lib.check(ctx, L.sph_get_fluid(ctx, vp(hx.data_ptr()), vp(hv.data_ptr()), vp(hp.data_ptr()), None, None))
     e2e_s = time.perf_counter() - t0
     s.close()
-    e2e_t = torch.tensor([e2e_s], device=dev)
-    if dist:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world * K / float(e2e_t.item())
+    e2e_value = world * K / ranks.max_over_ranks(e2e_s, dist, dev)
     h2d = 24 * n + (4 * n if headline != "zero" else 0)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = run_cpu_reference(budget_s=20.0, max_steps=K)
+        cpu = run_cpu_reference(budget_s=15.0, max_steps=K)
 
     if rank == 0:
         line = {
@@ -371,32 +396,54 @@ def bench_ours(args):
 def bench_batched(args):
     """64 independent dam breaks (log-uniform 5k-200k particles) advanced in
     one batch, launch shapes from the autotuner, versus the same scenes solved
-    one context at a time.  Prints its own JSON line."""
+    one context at a time.  Under torchrun the scenes are sharded over the
+    ranks by particle count (strong scaling: the 64-scene step is the unit);
+    the step time is the slowest rank's.  Prints its own JSON line."""
     import torch
 
     from warpsph_b200 import autotune as at
+    from warpsph_b200 import ranks
     from warpsph_b200.batch import BatchIISPH
     from warpsph_b200.params import SolverParams
     from warpsph_b200.scenes import batched_scenes
     from warpsph_b200.solver import IISPH
 
-    scenes = batched_scenes()
+    rank, world, local = ranks.env_rank()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = ranks.init("nccl", device=dev)
+    all_scenes = batched_scenes()
+    n_all = sum(s.n for s in all_scenes)
+    mine = ranks.partition_scenes([s.n for s in all_scenes], world)[rank]
+    scenes = [all_scenes[k] for k in mine]
     n = sum(s.n for s in scenes)
     params = SolverParams(diameter=0.01, gravity=9.81, w_table_size=1024, g_table_size=1024,
-                          warm_start=args.warm if args.warm != "mlp" else "mlp")
+                          warm_start=args.warm, device=local)
     tuned = at.autotune(scenes, params, warm=10, steps=10)
     tp = at.apply(params, tuned)
     K = args.steps
     b = BatchIISPH(scenes, tp)
     b.prepare()
-    st = torch.cuda.ExternalStream(b._lib.sph_stream(b._ctx))
+    if args.warmup:
+        b.steps(args.warmup)
+    b.close()
+    b = BatchIISPH(scenes, tp)  # timed from the scenes' initial states
+    b.prepare()
+    st = torch.cuda.ExternalStream(b._lib.sph_stream(b._ctx), device=dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
     torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
     e0.record(st)
-    b._lib.sph_launch_steps(b._ctx, K)
+    rc = b._lib.sph_launch_steps(b._ctx, K)
     e1.record(st)
     e1.synchronize()
-    ms = e0.elapsed_time(e1)
+    clock = clocks.stop()
+    if rc != 0:
+        raise RuntimeError(f"sph_launch_steps failed ({rc})")
+    ms = ranks.max_over_ranks(e0.elapsed_time(e1), dist, dev)
     stats = b.scene_stats()
     b.close()
     # the same scenes, one context each, K steps each
@@ -404,7 +451,7 @@ def bench_batched(args):
     for sc in scenes:
         s = IISPH(stage_path=None, params=tp, scene=sc)
         s._lib.sph_prepare(s._ctx)
-        sst = torch.cuda.ExternalStream(s._lib.sph_stream(s._ctx))
+        sst = torch.cuda.ExternalStream(s._lib.sph_stream(s._ctx), device=dev)
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         a0.record(sst)
@@ -413,15 +460,24 @@ def bench_batched(args):
         a1.synchronize()
         seq_ms += a0.elapsed_time(a1)
         s.close()
-    line = {"metric": "batched IISPH steps/s (64 scenes per step)", "value": K / (ms / 1000.0), "unit": "steps/s",
-            "n_gpus": 1, "steps": K, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"64 dam breaks, {n} fluid particles in total, steps [0, {K})",
-                       "warm_start": params.warm_start},
-            "particle_updates_per_s": n * K / (ms / 1000.0),
-            "sequential_contexts_steps_per_s": K / (seq_ms / 1000.0),
-            "batch_speedup": seq_ms / ms, "autotuned": {k: v for k, v in tuned.items() if k != "trials"},
-            "last_step_iterations": {"min": int(stats["iterations"].min()), "max": int(stats["iterations"].max())}}
-    print(json.dumps(line), flush=True)
+    seq_ms = ranks.max_over_ranks(seq_ms, dist, dev)
+    if rank == 0:
+        line = {"metric": "batched IISPH steps/s (64 scenes per step)", "value": K / (ms / 1000.0),
+                "unit": "steps/s", "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": ms / K,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": f"64 dam breaks, {n_all} fluid particles in total, steps [0, {K})",
+                           "warm_start": params.warm_start, "parallelism": f"scenes sharded over {world}"},
+                "particle_updates_per_s": n_all * K / (ms / 1000.0),
+                "sequential_contexts_steps_per_s": K / (seq_ms / 1000.0),
+                "batch_speedup": seq_ms / ms, "autotuned_rank0": {k: v for k, v in tuned.items() if k != "trials"},
+                "last_step_iterations_rank0": {"min": int(stats["iterations"].min()),
+                                               "max": int(stats["iterations"].max())},
+                "clocks": clock}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def main():
