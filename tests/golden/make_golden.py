@@ -47,6 +47,12 @@ SCENES = {
     "compressed": dict(diameter=0.05, box=(0.5, 0.5, 0.5), gravity=9.8,
                        w_size=8192, g_size=65536, steps=3, jitter=2e-4, v0=(0.0, 0.0, 0.0),
                        isolated=False, compress=0.9, seed=2),
+    # The dam-break block with viscosity on (VIS_MU = 0.01 RHO_0, main.py:61):
+    # the laplacian of predict_v_adv (IISPH.py:248-278) acts on the jittered
+    # velocities from the first step.
+    "viscous": dict(diameter=0.02, box=(0.4, 0.24, 0.16), gravity=9.81,
+                    w_size=1024, g_size=1024, steps=3, jitter=1e-4, v0=(0.2, -0.5, 0.1),
+                    isolated=False, compress=1.0, seed=4, vis_mu_scale=0.01),
 }
 
 
@@ -88,7 +94,7 @@ def load_reference(ref: Path, cfg: dict):
     main.TIME_STEP_MAX = 5e-2 * d
     main.FLUID_MASS = main.RHO_0 * d**3
     main.SIGMA = 8 / (math.pi * main.SMOOTHING_LENGTH**3)
-    main.VIS_MU = 0.0 * main.RHO_0
+    main.VIS_MU = cfg.get("vis_mu_scale", 0.0) * main.RHO_0
     spkg = types.ModuleType("wp_sph_ref.solver")
     spkg.__path__ = [str(ref / "wp_sph" / "solver")]
     sys.modules["wp_sph_ref.solver"] = spkg
@@ -141,7 +147,7 @@ def run_scene(ref: Path, name: str, cfg: dict) -> dict:
             "scene": name, **{k: v for k, v in cfg.items() if k != "box"}, "box": list(cfg["box"]),
             "rho0": main.RHO_0, "omega": main.OMEGA, "eta": main.ETA, "inv_small": main.INV_SMALL,
             "h": main.SMOOTHING_LENGTH, "dt_max": main.TIME_STEP_MAX, "fluid_mass": main.FLUID_MASS,
-            "sigma": main.SIGMA, "n": sph.n, "boundary_n": sph.boundary_n,
+            "sigma": main.SIGMA, "vis_mu": main.VIS_MU, "n": sph.n, "boundary_n": sph.boundary_n,
             "generator": "tests/golden/make_golden.py (reference kernels under warp_emu)",
         }),
         "boundary_x": sph.boundary_x.numpy(),

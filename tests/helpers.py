@@ -11,6 +11,20 @@ def load_golden(name):
     return G, json.loads(str(G["meta"]))
 
 
+def golden_oracle_params(oracle, meta):
+    """Oracle constants of a golden scene (main.py:25-61 as make_golden patched them)."""
+    return oracle.reference_params(diameter=meta["diameter"], gravity=meta["gravity"], w_size=meta["w_size"],
+                                   g_size=meta["g_size"], vis_mu_scale=meta.get("vis_mu", 0.0) / meta["rho0"])
+
+
+def golden_solver_params(meta, **kw):
+    """SolverParams of a golden scene."""
+    from warpsph_b200.params import SolverParams
+
+    return SolverParams(diameter=meta["diameter"], gravity=meta["gravity"], w_table_size=meta["w_size"],
+                        g_table_size=meta["g_size"], vis_mu_scale=meta.get("vis_mu", 0.0) / meta["rho0"], **kw)
+
+
 def normrel(a, b):
     """max |a - b| / max |b|: the norm-wise relative error used by the parity bar."""
     a = np.asarray(a, np.float64)

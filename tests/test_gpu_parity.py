@@ -10,7 +10,7 @@ Bars (from the hot-path contract):
 import numpy as np
 import pytest
 
-from tests.helpers import csr_equal, load_golden, normrel
+from tests.helpers import csr_equal, golden_solver_params, load_golden, normrel
 
 pytestmark = pytest.mark.gpu
 
@@ -24,10 +24,7 @@ def _solver(params, scene):
 
 
 def _golden_params(meta, **kw):
-    from warpsph_b200.params import SolverParams
-
-    return SolverParams(diameter=meta["diameter"], gravity=meta["gravity"], w_table_size=meta["w_size"],
-                        g_table_size=meta["g_size"], keep_fb_lists=True, **kw)
+    return golden_solver_params(meta, keep_fb_lists=True, **kw)
 
 
 def _golden_scene(G, s):
@@ -37,7 +34,7 @@ def _golden_scene(G, s):
     return Scene(G[f"s{s}_x_in"], G[f"s{s}_v_in"], bx, len(bx), (0, 0, 0))
 
 
-@pytest.mark.parametrize("name", ["ref_lattice", "dam_jitter", "compressed"])
+@pytest.mark.parametrize("name", ["ref_lattice", "dam_jitter", "compressed", "viscous"])
 def test_golden_steps(name):
     G, meta = load_golden(name)
     sol = _solver(_golden_params(meta), _golden_scene(G, 0))
@@ -67,7 +64,7 @@ def test_golden_steps(name):
     sol.close()
 
 
-@pytest.mark.parametrize("name", ["dam_jitter", "compressed"])
+@pytest.mark.parametrize("name", ["dam_jitter", "compressed", "viscous"])
 def test_golden_fixed_iterations(name):
     """Pressure after exactly the reference's iteration count, even where the
     convergence test would stop one iteration apart."""
@@ -88,7 +85,7 @@ def _oracle_step(oracle, params, x, v, bx, psi, dt, inv_dt, precision="f32", **k
     from warpsph_b200.tables import kernel_tables
 
     op = oracle.reference_params(diameter=params.diameter, gravity=params.gravity, w_size=params.w_table_size,
-                                 g_size=params.g_table_size)
+                                 g_size=params.g_table_size, vis_mu_scale=params.vis_mu_scale)
     tabs = kernel_tables(params)
     if precision == "f64":
         tabs = oracle.kernel_tables(op, np.float64)
@@ -134,6 +131,41 @@ def test_dam_break_8k_vs_oracle(oracle):
             e_gpu = normrel(sol.rho.numpy(), truth["rho"])
             e_f32 = normrel(ref["rho"], truth["rho"])
             assert e_gpu < max(10 * e_f32, 1e-6)
+    sol.close()
+
+
+def test_viscous_dam_break_vs_oracle(oracle):
+    """Viscosity on (VIS_MU = 0.01 RHO_0): the three-pass build (lists and rho,
+    v_adv with the laplacian, advection terms) on the 8,000-particle dam break
+    after 40 steps of flow, one step against the FP32 oracle."""
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+
+    params = preset_params("dam_break_8k", keep_fb_lists=True, vis_mu_scale=0.01)
+    scene = preset_scene("dam_break_8k")
+    sol = _solver(params, scene)
+    psi = sol.boundary_phi.numpy()
+    sol.steps(40)
+    x, v = sol.x.numpy(), sol.v.numpy()
+    dt = sol.dt
+    ref = _oracle_step(oracle, params, x, v, scene.boundary_x, psi, dt, 1.0 / dt)
+    sol.set_state(x, v)
+    sol.set_dt(dt, 1.0 / dt)
+    sol.step()
+    nb = sol.get_neighbors(with_boundary=True)
+    assert csr_equal(nb["ff_off"], nb["ff_idx"], ref["ff_off"], ref["ff_idx"])
+    assert normrel(sol.rho.numpy(), ref["rho"]) < RTOL
+    assert normrel(sol.v_adv.numpy(), ref["v_adv"]) < RTOL
+    assert normrel(sol.rho_adv.numpy(), ref["rho_adv"]) < RTOL
+    assert normrel(sol.term_a_ii.numpy(), ref["a_ii"]) < RTOL
+    assert abs(sol.last_stats["iterations"] - ref["iterations"]) <= 1
+    if sol.last_stats["iterations"] == ref["iterations"]:
+        assert normrel(sol.p.numpy(), ref["p"]) < RTOL
+        assert normrel(sol.v.numpy(), ref["v"]) < RTOL
+    # the viscous term is really on: v_adv differs from v - g dt y
+    base = v.copy()
+    base[:, 1] -= params.gravity * dt
+    assert np.abs(sol.v_adv.numpy() - base).max() > 1e-3
     sol.close()
 
 

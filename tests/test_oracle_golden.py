@@ -4,16 +4,15 @@ runtime (tests/golden/make_golden.py).  No GPU needed."""
 import numpy as np
 import pytest
 
-from tests.helpers import csr_equal, load_golden, normrel
+from tests.helpers import csr_equal, golden_oracle_params, load_golden, normrel
 
-SCENES = ["ref_lattice", "dam_jitter", "compressed"]
+SCENES = ["ref_lattice", "dam_jitter", "compressed", "viscous"]
 
 
 @pytest.mark.parametrize("name", SCENES)
 def test_tables_bit_exact(oracle, name):
     G, meta = load_golden(name)
-    P = oracle.reference_params(diameter=meta["diameter"], gravity=meta["gravity"], w_size=meta["w_size"],
-                                g_size=meta["g_size"])
+    P = golden_oracle_params(oracle, meta)
     w, g = oracle.kernel_tables(P)
     assert np.array_equal(w, G["W_table"])
     assert np.array_equal(g, G["grad_W_table"])
@@ -22,8 +21,7 @@ def test_tables_bit_exact(oracle, name):
 @pytest.mark.parametrize("name", SCENES)
 def test_boundary_psi(oracle, name):
     G, meta = load_golden(name)
-    P = oracle.reference_params(diameter=meta["diameter"], gravity=meta["gravity"], w_size=meta["w_size"],
-                                g_size=meta["g_size"])
+    P = golden_oracle_params(oracle, meta)
     psi = oracle.boundary_psi(P, G["boundary_x"], tables=(G["W_table"], G["grad_W_table"]))
     assert normrel(psi, G["boundary_phi"]) < 1e-6
 
@@ -31,8 +29,7 @@ def test_boundary_psi(oracle, name):
 @pytest.mark.parametrize("name", SCENES)
 def test_steps_match_reference(oracle, name):
     G, meta = load_golden(name)
-    P = oracle.reference_params(diameter=meta["diameter"], gravity=meta["gravity"], w_size=meta["w_size"],
-                                g_size=meta["g_size"])
+    P = golden_oracle_params(oracle, meta)
     tabs = (G["W_table"], G["grad_W_table"])
     for s in range(int(G["steps"])):
         pre = f"s{s}_"
@@ -52,8 +49,7 @@ def test_steps_match_reference(oracle, name):
 def test_fp64_truth_close_to_fp32(oracle):
     """The FP32 mirror and the FP64 truth agree to float32 accuracy on a golden state."""
     G, meta = load_golden("dam_jitter")
-    P = oracle.reference_params(diameter=meta["diameter"], gravity=meta["gravity"], w_size=meta["w_size"],
-                                g_size=meta["g_size"])
+    P = golden_oracle_params(oracle, meta)
     args = (G["s0_x_in"], G["s0_v_in"], G["boundary_x"], None, G["boundary_phi"], float(G["s0_dt_in"]))
     r32 = oracle.step(P, *args, fixed_iters=8)
     r64 = oracle.step(P, *args, precision="f64", fixed_iters=8)

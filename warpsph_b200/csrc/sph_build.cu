@@ -6,12 +6,18 @@
 //   ELL list of fluid neighbours    count_same/store_same_neighbor (IISPH.py:52-104)
 //   fluid-boundary counts (+lists)  count_diff/store_diff_neighbor (IISPH.py:107-163)
 //   rho                             compute_density (IISPH.py:177-214)
-//   v_adv                           predict_v_adv (IISPH.py:217-278), VIS_MU = 0
+//   v_adv                           predict_v_adv (IISPH.py:217-278)
 //   rho_adv                         predict_rho_adv (IISPH.py:281-329)
 //   d_ii                            compute_term_d (IISPH.py:332-382)
 //   a_ii                            compute_term_a (IISPH.py:385-428)
 //   p for the first Jacobi pass     init_pressure + update_p (IISPH.py:166-174, 521-539)
 //   B_i = sum_b psi_b gradW_ib      the boundary sum reused by every Jacobi pass
+//
+// With VIS_MU = 0 (the reference's default, main.py:61) v_adv = v - g dt y is
+// local and everything above is one kernel (kBuildFull).  With viscosity,
+// v_adv needs the neighbours' densities and rho_adv the neighbours' v_adv, so
+// the step runs three list passes: kBuildLists (lists and rho), k_visc
+// (v_adv with the laplacian), kBuildAdvect (the rest, reading v_adv).
 //
 // Membership uses the reference's float32 test |x_i - x_j| < h (IISPH.py:71-72)
 // evaluated without contraction: r2 < r2_limit is exactly sqrt_rn(r2) < h.
@@ -65,24 +71,26 @@ __device__ inline int filter_rows(const Grid& g, int base, int3 ci, const int* _
   return cnt;
 }
 
-template <class Tab>
+template <int MODE, class Tab>
 __device__ __forceinline__ void build_body(const BuildArgs& a, const Tab& W, const Tab& G);
 
-template <bool SMEM>
+template <bool SMEM, int MODE>
 __global__ void __launch_bounds__(256) k_build(BuildArgs a) {
   extern __shared__ float2 s_pairs[];
   if (SMEM) {
     stage_pairs(s_pairs, a.w_table, a.c.sw);
     stage_pairs(s_pairs + a.c.sw, a.g_table, a.c.sg);
     __syncthreads();
-    build_body(a, PairTable{s_pairs}, PairTable{s_pairs + a.c.sw});
+    build_body<MODE>(a, PairTable{s_pairs}, PairTable{s_pairs + a.c.sw});
   } else {
-    build_body(a, FlatTable{a.w_table}, FlatTable{a.g_table});
+    build_body<MODE>(a, FlatTable{a.w_table}, FlatTable{a.g_table});
   }
 }
 
-template <class Tab>
+template <int MODE, class Tab>
 __device__ __forceinline__ void build_body(const BuildArgs& a, const Tab& W, const Tab& G) {
+  constexpr bool kLists = (MODE != kBuildAdvect);  // this pass builds the neighbour lists
+  constexpr bool kTerms = (MODE != kBuildLists);   // this pass writes the advection terms
   const Consts c = a.c;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = i < a.n;
@@ -91,18 +99,26 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Tab& W, con
     const CellFrame fr = frame_of(a.scenes, a.grid, false, i);
     const Grid& g = fr.g;
     const float dt = a.st->dt[fr.scene];
-    const float gdt = (-c.gravity) * dt;
+    // v_adv of particle i and the term added to a neighbour's v to get its
+    // v_adv: v - g dt y without viscosity, read back from k_visc with it
+    const float gdt = (MODE == kBuildAdvect) ? 0.f : (-c.gravity) * dt;
     const float4 xi = a.pos[i];
-    const float4 vi = a.vel[i];
-    const float vax = vi.x, vay = vi.y + gdt, vaz = vi.z;
+    const float4 vi = (MODE == kBuildAdvect) ? a.vadv[i] : a.vel[i];
+    const float4* vsrc = (MODE == kBuildAdvect) ? a.vadv : a.vel;
+    const float vax = vi.x, vay = (MODE == kBuildAdvect) ? vi.y : vi.y + gdt, vaz = vi.z;
     const int3 ci = cell_coord(g, xi.x, xi.y, xi.z);
     const int K = c.max_ff, KB = c.max_fb;
     int* nbr = a.nbr_ff + ell_index(i, 0, K);
     int* nbrb = a.nbr_fb + ell_index(i, 0, KB);
 
-    // phase 1: neighbour lists
-    cnt = filter_rows(g, fr.base, ci, a.cell_start, a.pos, xi, c.r2_limit, i, nbr, K);
-    if (a.nb > 0) cntb = filter_rows(g, fr.base, ci, a.bcell_start, a.bpos, xi, c.r2_limit, -1, nbrb, KB);
+    // phase 1: neighbour lists (the advect pass reads the lists built before)
+    if (kLists) {
+      cnt = filter_rows(g, fr.base, ci, a.cell_start, a.pos, xi, c.r2_limit, i, nbr, K);
+      if (a.nb > 0) cntb = filter_rows(g, fr.base, ci, a.bcell_start, a.bpos, xi, c.r2_limit, -1, nbrb, KB);
+    } else {
+      cnt = a.cnt_ff[i];
+      cntb = (a.nb > 0) ? a.cnt_fb[i] : 0;
+    }
 
     // phase 2: everything summed over the neighbours, in list (= ascending j) order
     float sW = 0.f, sGx = 0.f, sGy = 0.f, sGz = 0.f, sG2 = 0.f, div = 0.f;
@@ -127,14 +143,14 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Tab& W, con
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         xj[u] = __ldg(a.pos + j[u]);
-        vj[u] = __ldg(a.vel + j[u]);
+        vj[u] = __ldg(vsrc + j[u]);
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) fluid(xj[u], vj[u]);
     }
     for (; k < nf; ++k) {
       const int j = nbr[k * kWarp];
-      fluid(__ldg(a.pos + j), __ldg(a.vel + j));
+      fluid(__ldg(a.pos + j), __ldg(vsrc + j));
     }
 
     float sWb = 0.f, Bx = 0.f, By = 0.f, Bz = 0.f, divb = 0.f;
@@ -187,17 +203,21 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Tab& W, con
     }
 
     a.rho[i] = rho;
-    a.bvec[i] = make_float4(Bx, By, Bz, rho_adv);
-    a.dii_aii[i] = make_float4(dix, diy, diz, aii);
-    a.vadv[i] = make_float4(vax, vay, vaz, 0.f);
-    if (c.warm_start != SPH_WARM_MLP) {
-      a.p0[i] = p;
-      a.P4[i] = make_float4(dix * p, diy * p, diz * p, p / rr);
+    if (kLists) {
+      a.cnt_ff[i] = cnt;
+      if (a.cnt_fb) a.cnt_fb[i] = cntb;
     }
-    a.cnt_ff[i] = cnt;
-    if (a.cnt_fb) a.cnt_fb[i] = cntb;
+    if (kTerms) {
+      a.bvec[i] = make_float4(Bx, By, Bz, rho_adv);
+      a.dii_aii[i] = make_float4(dix, diy, diz, aii);
+      if (MODE == kBuildFull) a.vadv[i] = make_float4(vax, vay, vaz, 0.f);
+      if (c.warm_start != SPH_WARM_MLP) {
+        a.p0[i] = p;
+        a.P4[i] = make_float4(dix * p, diy * p, diz * p, p / rr);
+      }
+    }
 
-    if (a.feat) {
+    if (kTerms && a.feat) {
       // Learned warm-start inputs (kFeatures per particle, dimensionless; the
       // network standardises them with its own mean / std).  Pressures span
       // orders of magnitude, so they enter as asinh(p / (rho0 g h)).
@@ -221,7 +241,8 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Tab& W, con
       f[9] = float(cntb);                                      // boundary neighbour count
     }
   }
-  // bookkeeping: overflow flags, pair totals, max counts
+  // bookkeeping: overflow flags, pair totals, max counts (once per step)
+  if (!kLists) return;
   const unsigned int full = 0xffffffffu;
   int over = live ? ((cnt > c.max_ff ? SPH_F_FF_OVERFLOW : 0) | (cntb > c.max_fb ? SPH_F_FB_OVERFLOW : 0)) : 0;
   unsigned long long pf = warp_sum((unsigned long long)cnt);
@@ -234,6 +255,81 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Tab& W, con
     atomicMax(&a.acc->max_ff, mf);
     atomicMax(&a.acc->max_fb, mb);
     if (over) atomicOr(&a.acc->flags, over);
+  }
+}
+
+// predict_v_adv with viscosity (IISPH.py:217-278), after kBuildLists wrote
+// the lists and every density:
+//   term_1 = -sum_j gradW_ij ((v_i - v_j) . x_ij) / rho_j / r_ij^2
+//   term_2 = -sum_b gradW_ib psi_b (v_i . x_ib) / r_ib^2
+//   v_adv  = v + (10 (m term_1 + term_2 / rho0) mu / rho_i - g y) dt
+// with x_ij = x_j - x_i and r the float32 length the list test used; the
+// operations keep the reference's order (vector * scalar, then each division).
+template <class Tab>
+__device__ __forceinline__ void visc_body(const BuildArgs& a, const Tab& G) {
+  const Consts c = a.c;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const CellFrame fr = frame_of(a.scenes, a.grid, false, i);
+  const float dt = a.st->dt[fr.scene];
+  const float4 xi = a.pos[i];
+  const float4 vi = a.vel[i];
+  const int K = c.max_ff, KB = c.max_fb;
+  const int* nbr = a.nbr_ff + ell_index(i, 0, K);
+  const int nf = min(a.cnt_ff[i], K);
+  float t1x = 0.f, t1y = 0.f, t1z = 0.f;
+  for (int k = 0; k < nf; ++k) {
+    const int j = nbr[k * kWarp];
+    const float4 xj = __ldg(a.pos + j);
+    const float4 vj = __ldg(a.vel + j);
+    const float rj = __ldg(a.rho + j);
+    const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+    const float r = __fsqrt_rn(dist2_rn(xi.x, xi.y, xi.z, xj.x, xj.y, xj.z));
+    const float gs = grad_scalar(G, r, c);
+    const float dot = __fadd_rn(__fadd_rn(__fmul_rn(vi.x - vj.x, dx), __fmul_rn(vi.y - vj.y, dy)),
+                                __fmul_rn(vi.z - vj.z, dz));
+    const float r2 = __fmul_rn(r, r);
+    t1x -= __fdiv_rn(__fdiv_rn(__fmul_rn(__fmul_rn(gs, dx), dot), rj), r2);
+    t1y -= __fdiv_rn(__fdiv_rn(__fmul_rn(__fmul_rn(gs, dy), dot), rj), r2);
+    t1z -= __fdiv_rn(__fdiv_rn(__fmul_rn(__fmul_rn(gs, dz), dot), rj), r2);
+  }
+  float t2x = 0.f, t2y = 0.f, t2z = 0.f;
+  if (a.nb > 0) {
+    const int* nbrb = a.nbr_fb + ell_index(i, 0, KB);
+    const int nbh = min(a.cnt_fb[i], KB);
+    for (int t = 0; t < nbh; ++t) {
+      const int b = nbrb[t * kWarp];
+      const float4 xb = __ldg(a.bpos + b);
+      const float dx = xb.x - xi.x, dy = xb.y - xi.y, dz = xb.z - xi.z;
+      const float r = __fsqrt_rn(dist2_rn(xi.x, xi.y, xi.z, xb.x, xb.y, xb.z));
+      const float gs = grad_scalar(G, r, c);
+      const float dot = __fadd_rn(__fadd_rn(__fmul_rn(vi.x, dx), __fmul_rn(vi.y, dy)), __fmul_rn(vi.z, dz));
+      const float r2 = __fmul_rn(r, r);
+      t2x -= __fdiv_rn(__fmul_rn(__fmul_rn(__fmul_rn(gs, dx), xb.w), dot), r2);
+      t2y -= __fdiv_rn(__fmul_rn(__fmul_rn(__fmul_rn(gs, dy), xb.w), dot), r2);
+      t2z -= __fdiv_rn(__fmul_rn(__fmul_rn(__fmul_rn(gs, dz), xb.w), dot), r2);
+    }
+  }
+  const float ri = a.rho[i];
+  const float lx = 10.f * __fadd_rn(__fmul_rn(t1x, c.m), __fdiv_rn(t2x, c.rho0));
+  const float ly = 10.f * __fadd_rn(__fmul_rn(t1y, c.m), __fdiv_rn(t2y, c.rho0));
+  const float lz = 10.f * __fadd_rn(__fmul_rn(t1z, c.m), __fdiv_rn(t2z, c.rho0));
+  const float ax = __fdiv_rn(__fmul_rn(lx, c.mu), ri);
+  const float ay = __fadd_rn(__fdiv_rn(__fmul_rn(ly, c.mu), ri), -c.gravity);
+  const float az = __fdiv_rn(__fmul_rn(lz, c.mu), ri);
+  a.vadv[i] = make_float4(__fadd_rn(vi.x, __fmul_rn(ax, dt)), __fadd_rn(vi.y, __fmul_rn(ay, dt)),
+                          __fadd_rn(vi.z, __fmul_rn(az, dt)), 0.f);
+}
+
+template <bool SMEM>
+__global__ void __launch_bounds__(256) k_visc(BuildArgs a) {
+  extern __shared__ float2 s_pairs[];
+  if (SMEM) {
+    stage_pairs(s_pairs, a.g_table, a.c.sg);
+    __syncthreads();
+    visc_body(a, PairTable{s_pairs});
+  } else {
+    visc_body(a, FlatTable{a.g_table});
   }
 }
 
@@ -269,18 +365,45 @@ __global__ void k_pack_psi(int nb, const float* __restrict__ psi, float4* bpos) 
 static size_t table_bytes(const Consts& c) { return sizeof(float2) * (size_t(c.sw) + size_t(c.sg)); }
 static bool tables_fit_smem(const Consts& c) { return table_bytes(c) <= 96 * 1024; }
 
-cudaError_t launch_build(const BuildArgs& a, int block, cudaStream_t s) {
-  if (a.n <= 0) return cudaSuccess;
-  const int grid = (a.n + block - 1) / block;
+template <int MODE>
+static cudaError_t launch_build_mode(const BuildArgs& a, int grid, int block, cudaStream_t s) {
   if (tables_fit_smem(a.c)) {
     const size_t smem = table_bytes(a.c);
     if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k_build<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+      cudaError_t e =
+          cudaFuncSetAttribute(k_build<true, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
       if (e != cudaSuccess) return e;
     }
-    k_build<true><<<grid, block, smem, s>>>(a);
+    k_build<true, MODE><<<grid, block, smem, s>>>(a);
   } else {
-    k_build<false><<<grid, block, 0, s>>>(a);
+    k_build<false, MODE><<<grid, block, 0, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_build(const BuildArgs& a, int block, int mode, cudaStream_t s) {
+  if (a.n <= 0) return cudaSuccess;
+  const int grid = (a.n + block - 1) / block;
+  switch (mode) {
+    case kBuildFull: return launch_build_mode<kBuildFull>(a, grid, block, s);
+    case kBuildLists: return launch_build_mode<kBuildLists>(a, grid, block, s);
+    case kBuildAdvect: return launch_build_mode<kBuildAdvect>(a, grid, block, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_visc(const BuildArgs& a, int block, cudaStream_t s) {
+  if (a.n <= 0) return cudaSuccess;
+  const int grid = (a.n + block - 1) / block;
+  const size_t smem = sizeof(float2) * size_t(a.c.sg);
+  if (smem <= 96 * 1024) {
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k_visc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+      if (e != cudaSuccess) return e;
+    }
+    k_visc<true><<<grid, block, smem, s>>>(a);
+  } else {
+    k_visc<false><<<grid, block, 0, s>>>(a);
   }
   return cudaGetLastError();
 }

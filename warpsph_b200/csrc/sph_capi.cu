@@ -497,7 +497,15 @@ int enqueue_front(SphCtx* ctx) {
   CK(sph::launch_gather(int(ctx->n), ctx->sort_src, ctx->sort_orig, ctx->pos_s, ctx->vel_s, ctx->p_s, ctx->pos_w,
                         ctx->vel_w, ctx->orig_w, ctx->pprev_w, ctx->stream));
   int block = ctx->P.block_size > 0 ? ctx->P.block_size : 128;
-  CK(sph::launch_build(build_args(ctx), block, ctx->stream));
+  const sph::BuildArgs b = build_args(ctx);
+  if (ctx->P.vis_mu == 0.0) {
+    CK(sph::launch_build(b, block, sph::kBuildFull, ctx->stream));
+  } else {
+    // viscosity: v_adv needs every density, rho_adv every v_adv (three passes)
+    CK(sph::launch_build(b, block, sph::kBuildLists, ctx->stream));
+    CK(sph::launch_visc(b, block, ctx->stream));
+    CK(sph::launch_build(b, block, sph::kBuildAdvect, ctx->stream));
+  }
   return SPH_OK;
 }
 
@@ -709,7 +717,7 @@ int sph_create(const SphParams* params, SphCtx** out) {
   if (!(P.h > 0) || !(P.rho0 > 0) || P.w_table_size < 2 || P.g_table_size < 2 || P.max_ff < 1 || P.max_fb < 1 ||
       !(P.dt0 > 0) || !(P.dt_max > 0))
     return SPH_E_INVALID;
-  if (P.vis_mu != 0.0) return SPH_E_INVALID;  // viscosity is not built: VIS_MU = 0 in the reference
+  if (!(P.vis_mu >= 0.0)) return SPH_E_INVALID;
   SphCtx* ctx = new SphCtx();
   ctx->P = P;
   if (ctx->P.timeout_ms <= 0) ctx->P.timeout_ms = 2000;

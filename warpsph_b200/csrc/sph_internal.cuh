@@ -351,7 +351,11 @@ struct PsiArgs {
 
 // launchers (host)
 cudaError_t launch_sort(const SortArgs& a, int ncells, cudaStream_t s);
-cudaError_t launch_build(const BuildArgs& a, int block, cudaStream_t s);
+// neighbour-build passes: one fused pass without viscosity, or lists + rho,
+// then launch_visc (v_adv), then the advection terms
+constexpr int kBuildFull = 0, kBuildLists = 1, kBuildAdvect = 2;
+cudaError_t launch_build(const BuildArgs& a, int block, int mode, cudaStream_t s);
+cudaError_t launch_visc(const BuildArgs& a, int block, cudaStream_t s);
 cudaError_t launch_psi(const PsiArgs& a, int block, cudaStream_t s);
 cudaError_t launch_psi_sorted(const PsiArgs& a, float* psi_sorted, int block, cudaStream_t s);
 cudaError_t launch_gather(int n, const int* sort_src, const int* sort_orig, const float4* pos_in,
