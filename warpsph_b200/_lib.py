@@ -58,7 +58,8 @@ class SphParams(ctypes.Structure):
         ("max_ff", ctypes.c_int32), ("max_fb", ctypes.c_int32), ("keep_fb_lists", ctypes.c_int32),
         ("use_graph", ctypes.c_int32), ("device", ctypes.c_int32), ("block_size", ctypes.c_int32),
         ("timeout_ms", ctypes.c_int32), ("jacobi_block", ctypes.c_int32), ("jacobi_ppt", ctypes.c_int32),
-        ("jacobi_unroll", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2),
+        ("jacobi_unroll", ctypes.c_int32), ("move_boundary", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 1),
     ]
 
 

@@ -49,6 +49,9 @@ struct SphCtx {
   float4* bpos = nullptr;
   float4* bvel = nullptr;
   int* borig = nullptr;
+  // per-step re-sort of a moving boundary (move_boundary): keys and temporaries
+  float4 *bpos_t = nullptr, *bvel_t = nullptr;
+  int *borig_t = nullptr, *bkey = nullptr, *brank = nullptr, *bsrc = nullptr;
   int* bcell_start = nullptr;
 
   // fluid
@@ -322,6 +325,35 @@ int set_grid(SphCtx* ctx, const float* xf, int64_t n) {
 }
 
 // Sort the boundary into the grid and compute psi (compute_boundary_density).
+// The boundary moves every step: requested, and some boundary velocity is nonzero.
+bool boundary_moves(const SphCtx* ctx) { return ctx->P.move_boundary && ctx->b_moving && ctx->nb > 0; }
+
+// Re-sort the (moved) boundary into the grid on the device, carrying psi in
+// bpos.w: the per-step boundary_grid.build of a dynamic scene (IISPH.py:1415-1416).
+int enqueue_boundary_resort(SphCtx* ctx) {
+  const int64_t nb = ctx->nb;
+  sph::SortArgs s{};
+  s.n = int(nb);
+  s.grid = ctx->grids[0];
+  s.scenes = ctx->d_scenes;
+  s.boundary = 1;
+  s.pos = ctx->bpos;
+  s.orig = ctx->borig;
+  s.key = ctx->bkey;
+  s.rank = ctx->brank;
+  s.cell_count = ctx->cell_count;
+  s.cell_start = ctx->bcell_start;
+  s.scan_part = ctx->scan_part;
+  s.sort_src = ctx->bsrc;
+  s.sort_orig = ctx->borig_t;
+  CK(sph::launch_sort(s, ctx->total_cells, ctx->stream));
+  CK(sph::launch_gather(int(nb), ctx->bsrc, ctx->borig_t, ctx->bpos, ctx->bvel, nullptr, ctx->bpos_t, ctx->bvel_t,
+                        ctx->borig, nullptr, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->bpos, ctx->bpos_t, sizeof(float4) * nb, cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->bvel, ctx->bvel_t, sizeof(float4) * nb, cudaMemcpyDeviceToDevice, ctx->stream));
+  return SPH_OK;
+}
+
 int sort_boundary(SphCtx* ctx) {
   const int64_t nb = ctx->nb;
   const int nc = ctx->total_cells;
@@ -353,6 +385,14 @@ int sort_boundary(SphCtx* ctx) {
   CK(dalloc(ctx->borig, nb));
   if (ctx->b_moving) CK(dalloc(ctx->bvel, nb));
   else dfree(ctx->bvel);
+  if (boundary_moves(ctx)) {
+    CK(dalloc(ctx->bpos_t, nb));
+    CK(dalloc(ctx->bvel_t, nb));
+    CK(dalloc(ctx->borig_t, nb));
+    CK(dalloc(ctx->bkey, nb));
+    CK(dalloc(ctx->brank, nb));
+    CK(dalloc(ctx->bsrc, nb));
+  }
   sph::SortArgs s{};
   s.n = int(nb);
   s.grid = ctx->grids[0];
@@ -493,6 +533,10 @@ sph::BuildArgs build_args(SphCtx* ctx) {
 // sort + gather + build: everything up to the pressure solve
 int enqueue_front(SphCtx* ctx) {
   CK(cudaMemsetAsync(ctx->acc, 0, sizeof(StepAcc), ctx->stream));
+  if (boundary_moves(ctx)) {
+    const int rc = enqueue_boundary_resort(ctx);
+    if (rc) return rc;
+  }
   CK(sph::launch_sort(fluid_sort_args(ctx), ctx->total_cells, ctx->stream));
   CK(sph::launch_gather(int(ctx->n), ctx->sort_src, ctx->sort_orig, ctx->pos_s, ctx->vel_s, ctx->p_s, ctx->pos_w,
                         ctx->vel_w, ctx->orig_w, ctx->pprev_w, ctx->stream));
@@ -555,6 +599,10 @@ int enqueue_jacobi(SphCtx* ctx) {
   j.acc = ctx->acc;
   j.ring = ctx->ring;
   j.last = ctx->last;
+  j.bpos = ctx->bpos;
+  j.bvel = ctx->bvel;
+  j.nb = int(ctx->nb);
+  j.move_boundary = boundary_moves(ctx) ? 1 : 0;
   j.pos_out = ctx->pos_s;
   j.vel_out = ctx->vel_s;
   j.orig_out = ctx->orig_s;
@@ -775,7 +823,8 @@ void sph_destroy(SphCtx* ctx) {
   cudaSetDevice(ctx->dev);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
-  void* ptrs[] = {ctx->d_w, ctx->d_g, ctx->bpos, ctx->bvel, ctx->borig, ctx->bcell_start, ctx->pos_s, ctx->vel_s,
+  void* ptrs[] = {ctx->d_w, ctx->d_g, ctx->bpos, ctx->bvel, ctx->borig, ctx->bpos_t, ctx->bvel_t, ctx->borig_t,
+                  ctx->bkey, ctx->brank, ctx->bsrc, ctx->bcell_start, ctx->pos_s, ctx->vel_s,
                   ctx->pos_w, ctx->vel_w, ctx->orig_s, ctx->orig_w, ctx->p_s, ctx->pprev_w, ctx->key, ctx->rank,
                   ctx->sort_src, ctx->sort_orig, ctx->cell_count, ctx->cell_start, ctx->scan_part, ctx->nbr_ff,
                   ctx->cnt_ff, ctx->nbr_fb, ctx->cnt_fb, ctx->rho, ctx->bvec, ctx->dii_aii, ctx->vadv, ctx->P4,

@@ -329,6 +329,9 @@ struct JacobiArgs {
   StepAcc* acc;
   SphStepStats* ring;      // per-step stats ring buffer
   SphStepStats* last;      // stats of the last completed step
+  float4* bpos;            // sorted boundary (x, y, z, psi), moved by v dt after the drift
+  const float4* bvel;
+  int nb, move_boundary;
   // outputs of the kick/drift epilogue (next step's state)
   float4* pos_out;
   float4* vel_out;

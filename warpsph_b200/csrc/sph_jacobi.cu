@@ -353,6 +353,20 @@ __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G) {
       }
     }
     if (run >= 0) flush();
+    if (a.move_boundary) {
+      // update_rigid_x (IISPH.py:651-671): x_b += v_b dt with the step's dt
+      // (the last block replaces dt only after every block has finished here)
+      for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < a.nb; b += gridDim.x * blockDim.x) {
+        const int s = (a.nscenes == 1) ? 0 : find_scene(a.scenes->bound_off, a.nscenes, b);
+        const float dt = a.st->dt[s];
+        float4 xb = a.bpos[b];
+        const float4 vb = __ldg(a.bvel + b);
+        xb.x = __fadd_rn(xb.x, __fmul_rn(vb.x, dt));
+        xb.y = __fadd_rn(xb.y, __fmul_rn(vb.y, dt));
+        xb.z = __fadd_rn(xb.z, __fmul_rn(vb.z, dt));
+        a.bpos[b] = xb;
+      }
+    }
   }
   const int nonfinite = __syncthreads_or(!finite);
   if (threadIdx.x == 0) {

@@ -43,6 +43,7 @@ class SolverParams:
     jacobi_block: int = 0         # pressure solve threads per block (0 = 256)
     jacobi_ppt: int = 0           # particles per solve thread (0 = 1)
     jacobi_unroll: int = 0        # solve neighbour-loop unroll (0 = 2)
+    move_boundary: bool = False   # boundary moves with its velocities (DYNAMIC_SCENE, main.py:20)
     dt0: float | None = None      # None: TIME_STEP_MAX (IISPH.py:747)
     domain_min: tuple = (0.0, 0.0, 0.0)
     domain_max: tuple = (0.0, 0.0, 0.0)
@@ -110,6 +111,7 @@ class SolverParams:
         p.jacobi_block = self.jacobi_block
         p.jacobi_ppt = self.jacobi_ppt
         p.jacobi_unroll = self.jacobi_unroll
+        p.move_boundary = int(self.move_boundary)
         return p
 
     @classmethod

@@ -101,6 +101,44 @@ def dam_break(fluid=(20, 20, 20), spacing=0.02, box=(1.0, 0.6, 0.4), jitter=1e-4
                  boundary_x=b.astype(np.float32), boundary_hide_n=len(b), box=tuple(box))
 
 
+def box_surface(lo, hi, spacing) -> np.ndarray:
+    """Particles on the six faces of the box [lo, hi]: every lattice point
+    lo + k * spacing (k >= 0, up to hi) with at least one coordinate on a face,
+    ordered x, y, z (z fastest)."""
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    n = [int(np.floor((h - l) / spacing + 1e-9)) + 1 for l, h in zip(lo, hi)]
+    ix, iy, iz = (a.ravel() for a in np.meshgrid(*[np.arange(k) for k in n], indexing="ij"))
+    face = (ix == 0) | (ix == n[0] - 1) | (iy == 0) | (iy == n[1] - 1) | (iz == 0) | (iz == n[2] - 1)
+    pts = lo + spacing * np.stack([ix[face], iy[face], iz[face]], axis=1)
+    return pts.astype(np.float32)
+
+
+def torus_surface(center, major, minor, spacing, axis=1) -> np.ndarray:
+    """Particles on a torus surface: a tube of radius ``minor`` around a circle
+    of radius ``major`` in the plane normal to ``axis`` (0, 1, 2 = x, y, z),
+    about ``spacing`` apart along the circle (at its centre line) and around
+    the tube."""
+    nu = max(8, int(round(2 * np.pi * major / spacing)))
+    nv = max(6, int(round(2 * np.pi * minor / spacing)))
+    u = 2 * np.pi * np.arange(nu) / nu
+    w = 2 * np.pi * np.arange(nv) / nv
+    uu, ww = (a.ravel() for a in np.meshgrid(u, w, indexing="ij"))
+    ring = major + minor * np.cos(ww)
+    a, b, c = ring * np.cos(uu), minor * np.sin(ww), ring * np.sin(uu)  # b runs along the axis
+    local = {0: (b, a, c), 1: (a, b, c), 2: (a, c, b)}[axis]
+    pts = np.stack(local, axis=1) + np.asarray(center, np.float64)
+    return pts.astype(np.float32)
+
+
+def add_obstacles(scene: Scene, obstacles) -> Scene:
+    """Append obstacle boundary particles after the box walls (the walls stay
+    the first boundary_hide_n boundary particles, as in IISPH.py:927)."""
+    extra = [np.asarray(o, np.float32).reshape(-1, 3) for o in obstacles]
+    bx = np.concatenate([scene.boundary_x] + extra).astype(np.float32)
+    return Scene(scene.fluid_x, scene.fluid_v, bx, scene.boundary_hide_n, scene.box)
+
+
 def preset_scene(name: str) -> Scene:
     from .params import PRESETS
 

@@ -159,11 +159,25 @@ class IISPH:
         _lib.check(self._ctx, self._lib.sph_set_fluid(self._ctx, _lib.ptr(x), _lib.ptr(v), self.n))
 
     def set_boundary_velocity(self, vb):
-        """Boundary particle velocities (moving boundaries); re-uploads the boundary."""
+        """Boundary particle velocities (original order).  Re-uploads the
+        boundary at its current positions, which recomputes psi there."""
         self._boundary_v = np.ascontiguousarray(vb, dtype=np.float32).reshape(-1, 3)
-        b = np.ascontiguousarray(self._scene.boundary_x, dtype=np.float32)
+        b = np.ascontiguousarray(self.boundary_x.numpy(), dtype=np.float32)
         _lib.check(self._ctx, self._lib.sph_set_boundary(self._ctx, _lib.ptr(b), _lib.ptr(self._boundary_v),
                                                          self.boundary_n))
+
+    def set_rigid_velocity(self, v, start=None):
+        """set_rigid_v (IISPH.py:651-659): boundary particles [start, boundary_n)
+        (default: those after the box walls, boundary_hide_n) get velocity v.
+        With params.move_boundary they move by v dt after every step
+        (update_rigid_x, IISPH.py:662-671) and the boundary grid is rebuilt every
+        step.  The reference sets the velocity during its first step; call this
+        before the first step, so psi stays the one computed at start
+        (IISPH.py:811-821)."""
+        start = self.boundary_hide_n if start is None else int(start)
+        vb = self._boundary_v.copy()
+        vb[start:] = np.asarray(v, dtype=np.float32)
+        self.set_boundary_velocity(vb)
 
     def _create_context(self):
         cp = self.params.to_c()
