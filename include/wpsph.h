@@ -77,7 +77,7 @@ typedef struct SphParams {
   int32_t timeout_ms;    /* bound on every grid-wide wait */
   int32_t jacobi_block;  /* threads per block of the pressure solve: 128 or 256 (0 = 256) */
   int32_t jacobi_ppt;    /* particles per solve thread: 1 or 2 (0 = 1) */
-  int32_t jacobi_unroll; /* neighbour-loop unroll of the solve: 2, 4 or 8 (0 = 2) */
+  int32_t jacobi_unroll; /* neighbour-loop unroll of the solve: 2, 4 or 8 (0 = 4) */
   int32_t move_boundary;  /* 1: boundary particles move with their velocities, x += v dt after
                             every step's drift (update_rigid_x, IISPH.py:651-671, 1356-1365), and
                             the boundary grid is rebuilt every step (IISPH.py:1415-1416); psi

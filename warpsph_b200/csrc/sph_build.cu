@@ -10,7 +10,8 @@
 //   rho_adv                         predict_rho_adv (IISPH.py:281-329)
 //   d_ii                            compute_term_d (IISPH.py:332-382)
 //   a_ii                            compute_term_a (IISPH.py:385-428)
-//   p for the first Jacobi pass     init_pressure + update_p (IISPH.py:166-174, 521-539)
+//   p for the first Jacobi pass     init_pressure + update_p (IISPH.py:166-174, 521-539),
+//                                   and q = p / rho^2 in the position record's .w
 //   B_i = sum_b psi_b gradW_ib      the boundary sum reused by every Jacobi pass
 //
 // With VIS_MU = 0 (the reference's default, main.py:61) v_adv = v - g dt y is
@@ -199,7 +200,7 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Tab& W, con
     } else if (c.warm_start == SPH_WARM_HALF) {
       p = a.pprev[i] / 2.0f;
     } else {
-      p = 0.f;  // the learned warm start writes p_0 and P4 after the build
+      p = 0.f;  // the learned warm start writes p_0 and q_0 after the build
     }
 
     a.rho[i] = rho;
@@ -213,7 +214,9 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Tab& W, con
       if (MODE == kBuildFull) a.vadv[i] = make_float4(vax, vay, vaz, 0.f);
       if (c.warm_start != SPH_WARM_MLP) {
         a.p0[i] = p;
-        a.P4[i] = make_float4(dix * p, diy * p, diz * p, p / rr);
+        // q = p / rho^2 for the solve's first pass; only .w of the record is
+        // written, and other threads read only its .xyz in this kernel
+        reinterpret_cast<float*>(a.pos_q + i)[3] = p / rr;
       }
     }
 

@@ -64,7 +64,7 @@ struct SphCtx {
   int *cell_count = nullptr, *cell_start = nullptr, *scan_part = nullptr;
   int *nbr_ff = nullptr, *cnt_ff = nullptr, *nbr_fb = nullptr, *cnt_fb = nullptr;
   float* rho = nullptr;
-  float4 *bvec = nullptr, *dii_aii = nullptr, *vadv = nullptr, *P4 = nullptr, *s4 = nullptr;
+  float4 *bvec = nullptr, *dii_aii = nullptr, *vadv = nullptr, *a4 = nullptr;
   float *p_a = nullptr, *p_b = nullptr, *Ap = nullptr;
   float* pmlp = nullptr;
   float* feat = nullptr;             // learned warm-start inputs, kFeatures per particle
@@ -460,8 +460,7 @@ int alloc_fluid(SphCtx* ctx, int64_t n) {
   CK(dalloc(ctx->bvec, m));
   CK(dalloc(ctx->dii_aii, m));
   CK(dalloc(ctx->vadv, m));
-  CK(dalloc(ctx->P4, m));
-  CK(dalloc(ctx->s4, m));
+  CK(dalloc(ctx->a4, m));
   CK(dalloc(ctx->p_a, m));
   CK(dalloc(ctx->p_b, m));
   CK(dalloc(ctx->Ap, m));
@@ -472,7 +471,7 @@ int alloc_fluid(SphCtx* ctx, int64_t n) {
   CK(cudaMemset(ctx->bvec, 0, sizeof(float4) * m));
   CK(cudaMemset(ctx->dii_aii, 0, sizeof(float4) * m));
   CK(cudaMemset(ctx->vadv, 0, sizeof(float4) * m));
-  CK(cudaMemset(ctx->s4, 0, sizeof(float4) * m));
+  CK(cudaMemset(ctx->a4, 0, sizeof(float4) * m));
   CK(cudaMemset(ctx->Ap, 0, sizeof(float) * m));
   CK(cudaMemset(ctx->pmlp, 0, sizeof(float) * m));
   CK(cudaMemset(ctx->cnt_ff, 0, sizeof(int) * m));
@@ -525,7 +524,7 @@ sph::BuildArgs build_args(SphCtx* ctx) {
   b.dii_aii = ctx->dii_aii;
   b.vadv = ctx->vadv;
   b.p0 = ctx->p_a;
-  b.P4 = ctx->P4;
+  b.pos_q = ctx->pos_w;
   b.feat = (ctx->record_feat || ctx->P.warm_start == SPH_WARM_MLP) ? ctx->feat : nullptr;
   return b;
 }
@@ -560,11 +559,10 @@ int enqueue_warm(SphCtx* ctx) {
     m.n = ctx->n;
     m.w = ctx->mlp;
     m.feat = ctx->feat;
-    m.dii_aii = ctx->dii_aii;
     m.rho = ctx->rho;
     m.p_unit = float(ctx->P.rho0 * ctx->P.gravity * ctx->P.h);
     m.p0 = ctx->p_a;
-    m.P4 = ctx->P4;
+    m.pos_q = ctx->pos_w;
     CK(sph::launch_mlp_infer(m, ctx->sm_count, ctx->stream));
   }
   return SPH_OK;
@@ -591,8 +589,7 @@ int enqueue_jacobi(SphCtx* ctx) {
   j.orig_w = ctx->orig_w;
   j.p_a = ctx->p_a;
   j.p_b = ctx->p_b;
-  j.P4 = ctx->P4;
-  j.s4 = ctx->s4;
+  j.a4 = ctx->a4;
   j.Ap = ctx->Ap;
   j.partials = ctx->partials;
   j.st = ctx->st;
@@ -806,7 +803,7 @@ int sph_create(const SphParams* params, SphCtx** out) {
   if (cudaMemcpy(ctx->st, &s, sizeof(s), cudaMemcpyHostToDevice) != cudaSuccess) return bail(SPH_E_CUDA);
   ctx->jac_block = P.jacobi_block ? P.jacobi_block : 256;
   ctx->jac_ppt = P.jacobi_ppt ? P.jacobi_ppt : 1;
-  ctx->jac_unroll = P.jacobi_unroll ? P.jacobi_unroll : 2;
+  ctx->jac_unroll = P.jacobi_unroll ? P.jacobi_unroll : 4;
   if (!sph::jacobi_variant_ok(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll)) return bail(SPH_E_INVALID);
   ctx->chunk = ctx->jac_block * ctx->jac_ppt;
   if (sph::jacobi_config(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll, ctx->c.sg, &ctx->blocks_per_sm,
@@ -827,8 +824,8 @@ void sph_destroy(SphCtx* ctx) {
                   ctx->bkey, ctx->brank, ctx->bsrc, ctx->bcell_start, ctx->pos_s, ctx->vel_s,
                   ctx->pos_w, ctx->vel_w, ctx->orig_s, ctx->orig_w, ctx->p_s, ctx->pprev_w, ctx->key, ctx->rank,
                   ctx->sort_src, ctx->sort_orig, ctx->cell_count, ctx->cell_start, ctx->scan_part, ctx->nbr_ff,
-                  ctx->cnt_ff, ctx->nbr_fb, ctx->cnt_fb, ctx->rho, ctx->bvec, ctx->dii_aii, ctx->vadv, ctx->P4,
-                  ctx->s4, ctx->p_a, ctx->p_b, ctx->Ap, ctx->pmlp, ctx->feat, ctx->mlp, ctx->stage, ctx->partials, ctx->st, ctx->acc, ctx->ring,
+                  ctx->cnt_ff, ctx->nbr_fb, ctx->cnt_fb, ctx->rho, ctx->bvec, ctx->dii_aii, ctx->vadv, ctx->a4,
+                  ctx->p_a, ctx->p_b, ctx->Ap, ctx->pmlp, ctx->feat, ctx->mlp, ctx->stage, ctx->partials, ctx->st, ctx->acc, ctx->ring,
                   ctx->d_scenes, ctx->d_chunks, ctx->d_chunk_scene,
                   ctx->last};
   for (void* p : ptrs)
@@ -1112,7 +1109,18 @@ int sph_get_terms(SphCtx* ctx, float* d_ii3, float* a_ii, float* s3, float* v_ad
       for (int64_t k = 0; k < n; ++k) a_ii[ow[k]] = h[k].w;
   }
   if (s3) {
-    CK(cudaMemcpy(h.data(), ctx->s4, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    // the solve keeps a = d_ii p + s of the final iterate (the kick's term);
+    // s = a - d_ii p with the final p, which the step left in p_s in this order
+    std::vector<float4> d(n);
+    std::vector<float> p(n);
+    CK(cudaMemcpy(h.data(), ctx->a4, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(d.data(), ctx->dii_aii, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(p.data(), ctx->p_s, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    for (int64_t k = 0; k < n; ++k) {
+      h[k].x = std::fma(-d[k].x, p[k], h[k].x);
+      h[k].y = std::fma(-d[k].y, p[k], h[k].y);
+      h[k].z = std::fma(-d[k].z, p[k], h[k].z);
+    }
     put3(s3);
   }
   if (v_adv3) {

@@ -1,7 +1,10 @@
 // Internal structures and device helpers of libwpsph (sm_100a).
 //
 // Data layout (HBM), all in the cell-sorted particle order of the current step:
-//   pos  float4 (x, y, z, 0)          vel  float4 (vx, vy, vz, 0)
+//   pos  float4 (x, y, z, q)          vel  float4 (vx, vy, vz, 0)
+//        q = p / rho^2 of the current pressure iterate in the solve's work
+//        array (first written by the build or the warm-start network, then by
+//        every Jacobi update); the step's state arrays carry 0 there
 //   bpos float4 (x, y, z, psi)        boundary, sorted once
 //   nbr  int32, tile-major ELL: element k of particle i sits at
 //        (i/32)*32*K + k*32 + i%32, so a warp reading its k-th neighbours
@@ -184,6 +187,53 @@ __device__ __forceinline__ void stage_pairs(float2* dst, const float* __restrict
   for (int k = threadIdx.x; k < S - 1; k += blockDim.x) dst[k] = make_float2(T[k], T[k + 1]);
 }
 
+// The gradient table as the Jacobi passes read it: (T[k], T[k+1] - T[k])
+// pairs in shared memory, so an interpolation is one FMA, T[k] + a (T[k+1] -
+// T[k]); it differs from the reference's (1 - a) T[k] + a T[k+1] by rounding
+// only.  FlatSlopeTable is the same lookup on a table in global memory.
+struct SlopeTable {
+  const float2* P;
+  __device__ __forceinline__ float lerp(int lo, float a) const {
+    const float2 p = P[lo];
+    return fmaf(a, p.y, p.x);
+  }
+};
+struct FlatSlopeTable {
+  const float* T;
+  __device__ __forceinline__ float lerp(int lo, float a) const {
+    const float t0 = __ldg(T + lo);
+    return fmaf(a, __ldg(T + lo + 1) - t0, t0);
+  }
+};
+__device__ __forceinline__ void stage_slopes(float2* dst, const float* __restrict__ T, int S) {
+  for (int k = threadIdx.x; k < S - 1; k += blockDim.x) {
+    const float t0 = T[k];
+    dst[k] = make_float2(t0, T[k + 1] - t0);
+  }
+}
+
+// Scalar part of gradW for a listed neighbour (r < h by the list's exact
+// test) inside the Jacobi passes.  The reference's guards are not needed here:
+// at r = 0 the gradient's direction vector is zero, so the product is zero
+// whatever the table returns; an r that the approximate root rounds up to h
+// clamps to the last segment, whose end sample is 0; NaN converts to index 0.
+template <class Tab>
+__device__ __forceinline__ float grad_listed(const Tab& t, float r, float scale, int S) {
+  const float f = r * scale;
+  const int lo = min(__float2int_rz(f), S - 2);
+  return t.lerp(lo, f - float(lo));
+}
+
+// Square root for the kernel-table argument inside the Jacobi passes, where
+// the neighbour sets are already fixed.  The approximate instruction differs
+// from the rounded root by a few ulp, which moves a table lookup by ~1e-7
+// relative; the parity tests bound the effect on p.
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // Exact float32 |a-b|^2 as wp.length(a - b) squares it: no contraction,
 // x*x + y*y + z*z left to right.
 __device__ inline float dist2_rn(float ax, float ay, float az, float bx, float by, float bz) {
@@ -299,7 +349,7 @@ struct BuildArgs {
   float4* dii_aii;         // (d_ii, a_ii)
   float4* vadv;
   float* p0;               // initial pressure of the solve (p_1 for the zero warm start)
-  float4* P4;              // (d_ii p, p / rho^2)
+  float4* pos_q;           // the array `pos` points to: p0 / rho^2 goes into .w
   float* feat;             // optional MLP feature rows (n x 10), NULL to skip
 };
 
@@ -311,7 +361,7 @@ struct JacobiArgs {
   const SceneTable* scenes;
   Consts c;
   const float* g_table;
-  const float4* pos;
+  float4* pos;             // (x, y, z, q = p / rho^2): .w is rewritten by every update
   const int* nbr_ff;
   const int* cnt_ff;
   const float* rho;
@@ -321,8 +371,7 @@ struct JacobiArgs {
   const int* orig_w;
   float* p_a;              // ping
   float* p_b;              // pong
-  float4* P4;
-  float4* s4;              // (s, A1)
+  float4* a4;              // (d_ii p + s, 0): dt^2 times the pressure acceleration
   float* Ap;
   Partial* partials;       // one per chunk
   DevState* st;

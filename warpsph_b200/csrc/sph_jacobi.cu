@@ -6,16 +6,32 @@
 //       update_p; compute_term_Ap_1; compute_term_Ap_2; update_rho_error; loop += 1
 // with the error read on the host twice per iteration (IISPH.py:1489-1494).
 //
-// Here one iteration k is two grid-wide passes separated by barriers:
-//   pass A  s_k  = sum_j d_ij p_j            = -m dt^2 sum_j gradW_ij p_j / rho_j^2
-//           A1_k = m sum_j (d_ji p_i - d_jj p_j) . gradW_ij          (compute_term_Ap_1)
-//   pass B  Ap_k = A1_k + m sum_j (s_i - s_j) . gradW_ij + s_i . B_i + a_ii p_i
-//                                                                     (compute_term_Ap_2)
-//           err_k from rho_adv + Ap_k (update_rho_error), reduced in FP64 with a
-//           fixed order, and p_{k+1} = update_p(p_k, Ap_k) into the other buffer
+// The reference evaluates, with d_ij = -m dt^2 gradW_ij / rho_j^2 and
+// d_ji = m dt^2 gradW_ij / rho_i^2 (compute_term_d, IISPH.py:332-382),
+//   s_i  = sum_j d_ij p_j                                   (compute_term_Ap_1)
+//   Ap_i = m sum_j (d_ji p_i - d_jj p_j) . gradW_ij
+//        + m sum_j (s_i - s_j) . gradW_ij + s_i . B_i + a_ii p_i   (compute_term_Ap_2)
+// with B_i = sum_b psi_b gradW_ib.  Substituting a_ii (IISPH.py:385-428) and
+// d_ii (IISPH.py:382) and collecting terms gives the same value as
+//   a_i  = d_ii p_i + s_i
+//   Ap_i = m sum_j (a_i - a_j) . gradW_ij + a_i . B_i
+// (a_i is dt^2 times the pressure acceleration, the quantity the kick adds,
+// IISPH.py:684).  The pairwise differences a_i - a_j cancel the common part of
+// the field exactly, as s_i - s_j does in the reference.  Pass A needs only the
+// neighbours' positions and q_j = p_j / rho_j^2, which sit together in one
+// 16-byte record (pos.w); pass B needs their positions and a_j.  That is three
+// 16-byte gathers per neighbour per iteration instead of the four a direct
+// transcription needs (x and (d_jj p_j, q_j) in the first pass, x and s_j in
+// the second), and the gathers bound the passes.
+//
+// One iteration k is two grid-wide passes separated by barriers:
+//   pass A  s_k = -m dt^2 sum_j q_j gradW_ij,  a_k = d_ii p_k + s_k
+//   pass B  Ap_k, err_k from rho_adv + Ap_k (update_rho_error), reduced in FP64
+//           with a fixed order, and p_{k+1} = update_p(p_k, Ap_k) into the other
+//           buffer (and q_{k+1} into pos.w)
 // After the second barrier every block reduces the per-block partial sums in the
 // same order, so all blocks take the same convergence decision; the loop exits
-// with p_k and s_k exactly where the reference's does.  The zero warm start
+// with p_k and a_k exactly where the reference's does.  The zero warm start
 // begins at k = 1 because p_0 = 0 gives Ap_0 = 0 and the build already wrote p_1.
 //
 // Epilogue: kick (IISPH.py:674-688), drift (IISPH.py:691-699) written straight
@@ -25,88 +41,89 @@
 
 namespace sph {
 
-// Neighbour loops are unrolled by U with every load of a group issued before
-// any use, and the next group's indices are fetched while the current group's
-// gathers are in flight, so each thread keeps up to 2U independent loads
-// outstanding (the passes are bound by gather latency).
-// List entries are read once per pass with the streaming hint (ld.global.cs),
-// which lets the L2 keep the gathered pos / P4 / s4 arrays resident instead of
-// the list stream.  Positions and counts are read-only for the whole kernel and
-// use the non-coherent path; P4 and s4 are rewritten between barriers and use
-// plain coherent loads.
-template <int kUnroll, typename Body>
-__device__ __forceinline__ void for_neighbours(const int* nb, int cnt, const float4* pos, const float4* other,
-                                               Body body) {
-  int k = 0;
+// Neighbour loops run the same trip count on every lane of a warp (the
+// warp's largest neighbour count, rounded up to the unroll U) with no
+// divergent tail: a lane past its own count takes its own index, whose
+// gradient term is exactly zero (x_j = x_i).  Every load of a group is issued
+// before any use, and the next group's indices are fetched while the current
+// group's gathers are in flight, so each thread keeps up to 2U independent
+// loads outstanding.  List entries are read once per pass with the streaming
+// hint (ld.global.cs), which lets the L2 keep the gathered pos / a4 arrays
+// resident instead of the list stream.  pos (its .w) and a4 are rewritten
+// between barriers, so they are read with plain coherent loads.  NG = 1
+// gathers pos only, NG = 2 also the second array.
+template <int kUnroll, int NG, typename Body>
+__device__ __forceinline__ void for_neighbours(const int* __restrict__ nb, int cnt, int self,
+                                               const float4* pos, const float4* other, Body body) {
+  const int wmax = __reduce_max_sync(0xffffffffu, cnt);
   int jn[kUnroll];
-  if (cnt >= kUnroll) {
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) jn[u] = __ldcs(nb + u * kWarp);
-  }
-  for (; k + kUnroll <= cnt; k += kUnroll) {
+  for (int u = 0; u < kUnroll; ++u) jn[u] = (u < cnt) ? __ldcs(nb + u * kWarp) : self;
+  for (int k = 0; k < wmax; k += kUnroll) {
     int j[kUnroll];
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) j[u] = jn[u];
-    if (k + 2 * kUnroll <= cnt) {
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) jn[u] = __ldcs(nb + (k + kUnroll + u) * kWarp);
+    for (int u = 0; u < kUnroll; ++u) {
+      j[u] = jn[u];
+      const int kn = k + kUnroll + u;
+      jn[u] = (kn < cnt) ? __ldcs(nb + kn * kWarp) : self;
     }
     float4 xj[kUnroll], oj[kUnroll];
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
-      xj[u] = __ldg(pos + j[u]);
-      oj[u] = other[j[u]];
+      xj[u] = pos[j[u]];
+      if (NG == 2) oj[u] = other[j[u]];
     }
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) body(xj[u], oj[u]);
   }
-  for (; k < cnt; ++k) {
-    const int j = __ldcs(nb + k * kWarp);
-    body(__ldg(pos + j), other[j]);
-  }
 }
 
+// pass A for particle i: s = sum_j d_ij p_j (IISPH.py:458-464) and a = d_ii p + s.
+// Every lane of the warp calls it (live = false past the chunk's end, with i
+// a valid slot of the chunk), because the neighbour loop is warp-synchronous.
 template <int U, class Tab>
-__device__ inline void pass_a(int i, const JacobiArgs& a, const Tab& G, float t3) {
+__device__ inline void pass_a(int i, bool live, const JacobiArgs& a, const Tab& G, float t3, const float* pc) {
   const Consts& c = a.c;
-  const float4 xi = __ldg(a.pos + i);
-  const float4 qi = a.P4[i];
-  const float ci = t3 * qi.w;  // d_ji p_i = gradW_ij * (m dt^2 p_i / rho_i^2)
-  const int cnt = min(__ldg(a.cnt_ff + i), c.max_ff);
+  const float4 xi = a.pos[i];
+  const int cnt = live ? min(__ldg(a.cnt_ff + i), c.max_ff) : 0;
   const int* nb = a.nbr_ff + ell_index(i, 0, c.max_ff);
-  float sx = 0.f, sy = 0.f, sz = 0.f, a1 = 0.f;
-  for_neighbours<U>(nb, cnt, a.pos, a.P4, [&](const float4 xj, const float4 qj) {
+  float sx = 0.f, sy = 0.f, sz = 0.f;
+  // one gather per neighbour here against two in pass B: unroll twice as deep
+  // so both passes keep the same number of loads in flight
+  for_neighbours<(2 * U > 8 ? 8 : 2 * U), 1>(nb, cnt, i, a.pos, nullptr, [&](const float4 xj, const float4) {
     const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-    const float r = sqrtf(dx * dx + dy * dy + dz * dz);
-    const float gs = grad_scalar(G, r, c);
-    const float gx = gs * dx, gy = gs * dy, gz = gs * dz;
-    sx += gx * qj.w;
-    sy += gy * qj.w;
-    sz += gz * qj.w;
-    a1 += (ci * gx - qj.x) * gx + (ci * gy - qj.y) * gy + (ci * gz - qj.z) * gz;
+    const float gq = grad_listed(G, sqrt_approx(dx * dx + dy * dy + dz * dz), c.g_scale, c.sg) * xj.w;
+    sx = fmaf(gq, dx, sx);
+    sy = fmaf(gq, dy, sy);
+    sz = fmaf(gq, dz, sz);
   });
-  a.s4[i] = make_float4(-t3 * sx, -t3 * sy, -t3 * sz, a1 * c.m);
+  if (!live) return;
+  const float4 da = __ldg(a.dii_aii + i);
+  const float p = pc[i];
+  a.a4[i] = make_float4(da.x * p + (-t3 * sx), da.y * p + (-t3 * sy), da.z * p + (-t3 * sz), 0.f);
 }
 
+// pass B for particle i: Ap (compute_term_Ap_2, IISPH.py:469-518), the density
+// error (update_rho_error, IISPH.py:542-567) and p_{k+1} (update_p, IISPH.py:521-539)
 template <int U, class Tab>
-__device__ inline void pass_b(int i, const JacobiArgs& a, const Tab& G, const float* pc, float* pn,
+__device__ inline void pass_b(int i, bool live, const JacobiArgs& a, const Tab& G, const float* pc, float* pn,
                               double& es, long long& ec) {
   const Consts& c = a.c;
-  const float4 xi = __ldg(a.pos + i);
-  const float4 si = a.s4[i];
-  const int cnt = min(__ldg(a.cnt_ff + i), c.max_ff);
+  const float4 xi = a.pos[i];
+  const float4 ai = a.a4[i];
+  const int cnt = live ? min(__ldg(a.cnt_ff + i), c.max_ff) : 0;
   const int* nb = a.nbr_ff + ell_index(i, 0, c.max_ff);
   float acc = 0.f;
-  for_neighbours<U>(nb, cnt, a.pos, a.s4, [&](const float4 xj, const float4 sj) {
+  for_neighbours<U, 2>(nb, cnt, i, a.pos, a.a4, [&](const float4 xj, const float4 aj) {
     const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-    const float r = sqrtf(dx * dx + dy * dy + dz * dz);
-    const float gs = grad_scalar(G, r, c);
-    acc += (si.x - sj.x) * (gs * dx) + (si.y - sj.y) * (gs * dy) + (si.z - sj.z) * (gs * dz);
+    const float gs = grad_listed(G, sqrt_approx(dx * dx + dy * dy + dz * dz), c.g_scale, c.sg);
+    acc = fmaf(gs, (ai.x - aj.x) * dx + (ai.y - aj.y) * dy + (ai.z - aj.z) * dz, acc);
   });
+  if (!live) return;
   const float4 bv = __ldg(a.bvec + i);
   const float4 da = __ldg(a.dii_aii + i);
   const float p = pc[i];
-  const float Ap = si.w + ((acc * c.m + (si.x * bv.x + si.y * bv.y + si.z * bv.z)) + da.w * p);
+  const float Ap = acc * c.m + (ai.x * bv.x + ai.y * bv.y + ai.z * bv.z);
   // update_p (IISPH.py:534-539)
   float aa = da.w;
   if (aa > -c.inv_small && aa < c.inv_small) aa = (aa < 0.f ? -1.f : 1.f) * c.inv_small;
@@ -119,7 +136,7 @@ __device__ inline void pass_b(int i, const JacobiArgs& a, const Tab& G, const fl
   }
   const float rho = __ldg(a.rho + i);
   pn[i] = pnew;
-  a.P4[i] = make_float4(da.x * pnew, da.y * pnew, da.z * pnew, pnew / (rho * rho));
+  reinterpret_cast<float*>(a.pos + i)[3] = pnew / (rho * rho);
   a.Ap[i] = Ap;
 }
 
@@ -132,10 +149,10 @@ template <bool SMEM, int T, int PPT, int U>
 __global__ void __launch_bounds__(T) k_jacobi(JacobiArgs a) {
   extern __shared__ float2 s_pairs[];
   if (SMEM) {
-    stage_pairs(s_pairs, a.g_table, a.c.sg);
-    jacobi_body<T, PPT, U>(a, PairTable{s_pairs});
+    stage_slopes(s_pairs, a.g_table, a.c.sg);
+    jacobi_body<T, PPT, U>(a, SlopeTable{s_pairs});
   } else {
-    jacobi_body<T, PPT, U>(a, FlatTable{a.g_table});
+    jacobi_body<T, PPT, U>(a, FlatSlopeTable{a.g_table});
   }
 }
 
@@ -193,7 +210,7 @@ __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G) {
 #pragma unroll
       for (int q = 0; q < PPT; ++q) {
         const int i = r.x + q * T + threadIdx.x;
-        if (i < r.y) pass_a<U>(i, a, G, c.m * (dt * dt));
+        pass_a<U>(i < r.y ? i : r.x, i < r.y, a, G, c.m * (dt * dt), pc);
       }
     }
     if (!grid_barrier(acc, gridDim.x, a.budget)) { ok = false; break; }
@@ -230,7 +247,7 @@ __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G) {
 #pragma unroll
         for (int q = 0; q < PPT; ++q) {
           const int i = r.x + q * T + threadIdx.x;
-          if (i < r.y) pass_b<U>(i, a, G, pc, pn, es, ec);
+          pass_b<U>(i < r.y ? i : r.x, i < r.y, a, G, pc, pn, es, ec);
         }
       }
       if (run >= 0) flush();
@@ -309,7 +326,7 @@ __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G) {
     acc->final_buf[0] = (pc == a.p_a) ? 0 : 1;
   }
 
-  // kick + drift -> next step's state, with each scene's final p and s.  With
+  // kick + drift -> next step's state, with each scene's final p and a.  With
   // one scene every block knows the final buffer (pc); with several it is in
   // acc->final_buf, published by the last barrier.
   bool finite = true;
@@ -336,12 +353,11 @@ __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G) {
         const int i = r.x + q * T + threadIdx.x;
         if (i >= r.y) continue;
         const float4 va = a.vadv[i];
-        const float4 da = a.dii_aii[i];
-        const float4 sv = a.s4[i];
+        const float4 ak = a.a4[i];  // d_ii p + s of the final iterate
         const float p = pf[i];
-        const float vx = va.x + inv_dt * (da.x * p + sv.x);
-        const float vy = va.y + inv_dt * (da.y * p + sv.y);
-        const float vz = va.z + inv_dt * (da.z * p + sv.z);
+        const float vx = va.x + inv_dt * ak.x;
+        const float vy = va.y + inv_dt * ak.y;
+        const float vz = va.z + inv_dt * ak.z;
         const float4 x = a.pos[i];
         a.vel_out[i] = make_float4(vx, vy, vz, 0.f);
         a.pos_out[i] = make_float4(x.x + vx * dt, x.y + vy * dt, x.z + vz * dt, 0.f);

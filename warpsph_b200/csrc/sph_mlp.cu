@@ -145,8 +145,8 @@ __device__ __forceinline__ void feature_frag(const MlpSmem& s, const float* __re
 // ------------------------------------------------------------------ inference
 
 // The predicted pressure of every particle, written as the solve's first
-// iterate p_1 together with P4 = (d_ii p_1, p_1 / rho^2) for the first Jacobi
-// pass.  The network is residual on the previous step's pressure: with
+// iterate p_1 together with q_1 = p_1 / rho^2 (the .w of the particle's
+// position record) for the first Jacobi pass.  The network is residual on the previous step's pressure: with
 // u = asinh(p_prev / (rho0 g h)) (input 3, read here in float32, so the skip
 // path carries no bf16 rounding) the prediction is
 //   p_1 = sinh(max(u + min(y t_scale, kMaxRise), 0)) rho0 g h.
@@ -176,10 +176,9 @@ __global__ void __launch_bounds__(128) k_mlp_infer(MlpInferArgs a) {
           if (a.p0) {
             const float u = __ldg(a.feat + i * kFeatures + 3);
             const float p = sinhf(fmaxf(u + fminf(f.y[2 * h] * s.t_scale, kMaxRise), 0.f)) * a.p_unit;
-            const float4 da = __ldg(a.dii_aii + i);
             const float rho = __ldg(a.rho + i);
             a.p0[i] = p;
-            a.P4[i] = make_float4(da.x * p, da.y * p, da.z * p, p / (rho * rho));
+            reinterpret_cast<float*>(a.pos_q + i)[3] = p / (rho * rho);
           }
           if (a.pred) a.pred[i] = f.y[2 * h];
         }

@@ -50,11 +50,10 @@ struct MlpInferArgs {
   long long n;
   const MlpPacked* w;
   const float* feat;      // n x kFeatures, raw features
-  const float4* dii_aii;
   const float* rho;
   float p_unit;           // rho0 g h: pressure of one target unit
   float* p0;              // out: initial pressure
-  float4* P4;             // out: (d_ii p0, p0 / rho^2)
+  float4* pos_q;          // out: .w = p0 / rho^2 of each sorted position record
   float* pred;            // optional out: raw network output
 };
 

@@ -42,7 +42,7 @@ class SolverParams:
     timeout_ms: int = 2000
     jacobi_block: int = 0         # pressure solve threads per block (0 = 256)
     jacobi_ppt: int = 0           # particles per solve thread (0 = 1)
-    jacobi_unroll: int = 0        # solve neighbour-loop unroll (0 = 2)
+    jacobi_unroll: int = 0        # solve neighbour-loop unroll (0 = 4)
     move_boundary: bool = False   # boundary moves with its velocities (DYNAMIC_SCENE, main.py:20)
     dt0: float | None = None      # None: TIME_STEP_MAX (IISPH.py:747)
     domain_min: tuple = (0.0, 0.0, 0.0)
