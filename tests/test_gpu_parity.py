@@ -169,6 +169,41 @@ def test_viscous_dam_break_vs_oracle(oracle):
     sol.close()
 
 
+@pytest.mark.parametrize("g_size", [1024, 65536])
+def test_table_gradient_path(oracle, g_size):
+    """Gradient tables that are not the cubic spline's own samples (here one
+    sample nudged) make the solve interpolate the table, staged in shared
+    memory (1024 samples) or read from global memory (65536), instead of using
+    the closed form; both agree with the oracle run on the same tables."""
+    from warpsph_b200 import _lib
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+    from warpsph_b200.tables import kernel_tables
+
+    params = preset_params("dam_break_8k", g_table_size=g_size, fixed_iters=6)
+    scene = preset_scene("dam_break_8k")
+    warm = _solver(params.replace(fixed_iters=-1), scene)
+    warm.steps(20)
+    x, v, psi, dt = warm.x.numpy(), warm.v.numpy(), warm.boundary_phi.numpy(), warm.dt
+    warm.close()
+    w, g = kernel_tables(params)
+    g = g.copy()
+    g[-1] = np.nextafter(np.float32(0), np.float32(1))  # was exactly 0 at r = h
+    sol = _solver(params, scene)
+    _lib.check(sol._ctx, sol._lib.sph_set_tables(sol._ctx, _lib.ptr(w), len(w), _lib.ptr(g), len(g)))
+    sol.set_state(x, v)
+    sol.set_dt(dt, 1.0 / dt)
+    sol.step()
+    op = oracle.reference_params(diameter=params.diameter, gravity=params.gravity, w_size=params.w_table_size,
+                                 g_size=g_size)
+    ref = oracle.step(op, x, v, scene.boundary_x, None, psi, dt, 1.0 / dt, tables=(w, g), fixed_iters=6)
+    assert sol.last_stats["iterations"] == 6
+    assert normrel(sol.p.numpy(), ref["p"]) < RTOL
+    assert normrel(sol.term_Ap_i.numpy(), ref["Ap"]) < RTOL
+    assert normrel(sol.v.numpy(), ref["v"]) < RTOL
+    sol.close()
+
+
 def test_warm_start_half_vs_oracle(oracle):
     from warpsph_b200.params import preset_params
     from warpsph_b200.scenes import preset_scene

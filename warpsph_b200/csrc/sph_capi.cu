@@ -41,6 +41,9 @@ struct SphCtx {
   std::vector<float> w_host, g_host;
   float* d_w = nullptr;
   float* d_g = nullptr;
+  // the gradient table is the cubic spline's own (sampled as build_tables
+  // does): the solve may then evaluate the gradient in closed form
+  bool g_spline = true;
 
   // boundary (host copy in original order, to re-sort when the grid changes)
   int64_t nb = 0;
@@ -180,6 +183,11 @@ void make_consts(SphCtx* ctx) {
   c.max_ff = ctx->K_ff;
   c.max_fb = ctx->K_fb;
   c.keep_fb = P.keep_fb_lists;
+  const double sigma = P.sigma, h = P.h;
+  c.gi0 = float(12.0 * sigma / (h * h));
+  c.gi1 = float(18.0 * sigma / (h * h * h));
+  c.go = float(6.0 * sigma / (h * h * h));
+  c.h2q = float(h * h / 4.0);
 }
 
 int upload_tables(SphCtx* ctx) {
@@ -608,6 +616,7 @@ int enqueue_jacobi(SphCtx* ctx) {
   // or from the network (its prediction is used as the first iterate); the
   // 0.5 p_prev start runs the reference's extra Ap_0 evaluation (pass 0).
   j.start_iter = (ctx->P.warm_start == SPH_WARM_HALF) ? 0 : 1;
+  j.grad_spline = ctx->g_spline ? 1 : 0;
   j.budget = (long long)ctx->P.timeout_ms * (long long)ctx->clock_khz;
   j.dt_max = ctx->P.dt_max;
   j.cfl_len = ctx->P.cfl_len;
@@ -806,7 +815,7 @@ int sph_create(const SphParams* params, SphCtx** out) {
   ctx->jac_unroll = P.jacobi_unroll ? P.jacobi_unroll : 4;
   if (!sph::jacobi_variant_ok(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll)) return bail(SPH_E_INVALID);
   ctx->chunk = ctx->jac_block * ctx->jac_ppt;
-  if (sph::jacobi_config(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll, ctx->c.sg, &ctx->blocks_per_sm,
+  if (sph::jacobi_config(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll, ctx->c.sg, ctx->g_spline, &ctx->blocks_per_sm,
                          &ctx->jac_smem) != cudaSuccess ||
       ctx->blocks_per_sm < 1)
     return bail(SPH_E_CUDA);
@@ -843,10 +852,21 @@ int sph_set_tables(SphCtx* ctx, const float* w, int32_t nw, const float* g, int3
   CK(cudaSetDevice(ctx->dev));
   ctx->w_host.assign(w, w + nw);
   ctx->g_host.assign(g, g + ng);
+  {
+    // the closed-form gradient stands in for the table only if the table is
+    // exactly the cubic spline's, sampled as this library samples it
+    SphParams P2 = ctx->P;
+    P2.w_table_size = nw;
+    P2.g_table_size = ng;
+    std::vector<float> w2, g2;
+    build_tables(P2, w2, g2);
+    ctx->g_spline = g2.size() == size_t(ng) && std::memcmp(g2.data(), g, sizeof(float) * size_t(ng)) == 0;
+  }
   int rc = upload_tables(ctx);
   if (rc) return rc;
   int b = 0;
-  CK(sph::jacobi_config(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll, ctx->c.sg, &b, &ctx->jac_smem));
+  CK(sph::jacobi_config(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll, ctx->c.sg, ctx->g_spline, &b,
+                        &ctx->jac_smem));
   if (b < 1) return fail(ctx, SPH_E_CUDA, "jacobi kernel does not fit");
   if (b != ctx->blocks_per_sm) {
     ctx->blocks_per_sm = b;

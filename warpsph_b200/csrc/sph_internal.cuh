@@ -55,6 +55,9 @@ struct Consts {
   float eta;
   int min_iter, max_loop, fixed_iters, warm_start;
   int max_ff, max_fb, keep_fb;
+  // the cubic spline's gradient scalar -(dW/dr)/r in closed form:
+  // gi0 - gi1 r for r^2 <= h2q = h^2/4, go (h - r)^2 / r above
+  float gi0, gi1, go, h2q;
 };
 
 // Independent scenes solved together (batching).  Scene s owns fluid slots
@@ -182,6 +185,17 @@ __device__ __forceinline__ float grad_scalar(const Tab& T, float r, const Consts
   return table_lerp(T, r, c.g_scale, c.sg);
 }
 
+// Gradient scalar of the cubic spline (the function the gradient table
+// samples, sph_funcs.py:79-82) evaluated in closed form for a listed
+// neighbour, from r^2.  At r = 0 it returns the inner branch's finite value,
+// and the direction vector (zero) makes the term vanish.
+__device__ __forceinline__ float grad_spline(const Consts& c, float r2) {
+  const float ir = rsqrtf(fmaxf(r2, 1e-30f));
+  const float r = r2 * ir;
+  const float t = c.h - r;
+  return (r2 <= c.h2q) ? fmaf(-c.gi1, r, c.gi0) : c.go * t * t * ir;
+}
+
 // Stage a table into shared memory as (T[k], T[k+1]) pairs, k < S-1.
 __device__ __forceinline__ void stage_pairs(float2* dst, const float* __restrict__ T, int S) {
   for (int k = threadIdx.x; k < S - 1; k += blockDim.x) dst[k] = make_float2(T[k], T[k + 1]);
@@ -233,6 +247,23 @@ __device__ __forceinline__ float sqrt_approx(float x) {
   asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
   return r;
 }
+
+// The gradient scalar of a listed neighbour as the Jacobi passes evaluate it,
+// from r^2: in closed form when the gradient table is the cubic spline's own
+// (SplineGrad; it differs from the table's interpolation by at most 1.2e-6 of
+// the table's largest value at 1024 samples, and it needs no shared-memory
+// load, which the L1 data pipe bounding the passes would otherwise serve), else
+// from the table (TableGrad).
+struct SplineGrad {
+  __device__ __forceinline__ float operator()(const Consts& c, float r2) const { return grad_spline(c, r2); }
+};
+template <class Tab>
+struct TableGrad {
+  Tab t;
+  __device__ __forceinline__ float operator()(const Consts& c, float r2) const {
+    return grad_listed(t, sqrt_approx(r2), c.g_scale, c.sg);
+  }
+};
 
 // Exact float32 |a-b|^2 as wp.length(a - b) squares it: no contraction,
 // x*x + y*y + z*z left to right.
@@ -387,6 +418,7 @@ struct JacobiArgs {
   int* orig_out;
   float* p_out;
   int start_iter;          // 1: p_1 came from the build; 0: warm start, run pass 0
+  int grad_spline;         // 1: the gradient table is the cubic spline's (closed form in the passes)
   long long budget;        // barrier spin budget in SM cycles
   double dt_max, cfl_len, inv_small_d, eta_d;
 };
@@ -414,7 +446,7 @@ cudaError_t launch_gather(int n, const int* sort_src, const int* sort_orig, cons
                           const float4* vel_in, const float* p_in, float4* pos_out, float4* vel_out,
                           int* orig_out, float* p_out, cudaStream_t s);
 bool jacobi_variant_ok(int block, int ppt, int unroll);
-cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, int* blocks_per_sm, size_t* smem);
+cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, bool spline, int* blocks_per_sm, size_t* smem);
 cudaError_t launch_jacobi(const JacobiArgs& a, int grid, int block, int ppt, int unroll, size_t smem,
                           cudaStream_t s);
 cudaError_t launch_pack_fluid(int n, const float* x3, const float* v3, float4* pos, float4* vel, int* orig,

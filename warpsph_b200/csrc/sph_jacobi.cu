@@ -92,7 +92,7 @@ __device__ inline void pass_a(int i, bool live, const JacobiArgs& a, const Tab& 
   // so both passes keep the same number of loads in flight
   for_neighbours<(2 * U > 8 ? 8 : 2 * U), 1>(nb, cnt, i, a.pos, nullptr, [&](const float4 xj, const float4) {
     const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-    const float gq = grad_listed(G, sqrt_approx(dx * dx + dy * dy + dz * dz), c.g_scale, c.sg) * xj.w;
+    const float gq = G(c, dx * dx + dy * dy + dz * dz) * xj.w;
     sx = fmaf(gq, dx, sx);
     sy = fmaf(gq, dy, sy);
     sz = fmaf(gq, dz, sz);
@@ -116,7 +116,7 @@ __device__ inline void pass_b(int i, bool live, const JacobiArgs& a, const Tab& 
   float acc = 0.f;
   for_neighbours<U, 2>(nb, cnt, i, a.pos, a.a4, [&](const float4 xj, const float4 aj) {
     const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-    const float gs = grad_listed(G, sqrt_approx(dx * dx + dy * dy + dz * dz), c.g_scale, c.sg);
+    const float gs = G(c, dx * dx + dy * dy + dz * dz);
     acc = fmaf(gs, (ai.x - aj.x) * dx + (ai.y - aj.y) * dy + (ai.z - aj.z) * dz, acc);
   });
   if (!live) return;
@@ -143,16 +143,22 @@ __device__ inline void pass_b(int i, bool live, const JacobiArgs& a, const Tab& 
 template <int T, int PPT, int U, class Tab>
 __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G);
 
-// T threads per block, PPT particles per thread (chunks of T * PPT particles),
-// neighbour-loop unroll U: the knobs the autotuner chooses among.
-template <bool SMEM, int T, int PPT, int U>
+// How the passes get the kernel gradient: the table staged in shared memory,
+// the table in global memory (too large to stage), or the closed form.
+constexpr int kGradSmem = 0, kGradFlat = 1, kGradSpline = 2;
+
+// GM gradient mode, T threads per block, PPT particles per thread (chunks of
+// T * PPT particles), neighbour-loop unroll U: the knobs the autotuner chooses among.
+template <int GM, int T, int PPT, int U>
 __global__ void __launch_bounds__(T) k_jacobi(JacobiArgs a) {
   extern __shared__ float2 s_pairs[];
-  if (SMEM) {
+  if (GM == kGradSmem) {
     stage_slopes(s_pairs, a.g_table, a.c.sg);
-    jacobi_body<T, PPT, U>(a, SlopeTable{s_pairs});
+    jacobi_body<T, PPT, U>(a, TableGrad<SlopeTable>{SlopeTable{s_pairs}});
+  } else if (GM == kGradFlat) {
+    jacobi_body<T, PPT, U>(a, TableGrad<FlatSlopeTable>{FlatSlopeTable{a.g_table}});
   } else {
-    jacobi_body<T, PPT, U>(a, FlatSlopeTable{a.g_table});
+    jacobi_body<T, PPT, U>(a, SplineGrad{});
   }
 }
 
@@ -446,14 +452,17 @@ __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G) {
   }
 }
 
-static size_t jacobi_smem(int sg) { return (sg <= 8192) ? sizeof(float2) * size_t(sg) : 0; }
+static int grad_mode(int sg, bool spline) {
+  return spline ? kGradSpline : (sg <= 8192 ? kGradSmem : kGradFlat);
+}
+static size_t jacobi_smem(int mode, int sg) { return mode == kGradSmem ? sizeof(float2) * size_t(sg) : 0; }
 
 using JacobiKernel = void (*)(JacobiArgs);
 
-template <bool SMEM>
+template <int GM>
 static JacobiKernel pick_jacobi(int T, int ppt, int unroll) {
 #define SPH_JACOBI_CASE(T_, P_, U_) \
-  if (T == T_ && ppt == P_ && unroll == U_) return k_jacobi<SMEM, T_, P_, U_>;
+  if (T == T_ && ppt == P_ && unroll == U_) return k_jacobi<GM, T_, P_, U_>;
   SPH_JACOBI_CASE(128, 1, 2)
   SPH_JACOBI_CASE(128, 1, 4)
   SPH_JACOBI_CASE(128, 1, 8)
@@ -470,16 +479,23 @@ static JacobiKernel pick_jacobi(int T, int ppt, int unroll) {
   return nullptr;
 }
 
-static JacobiKernel jacobi_kernel(int sg, int T, int ppt, int unroll) {
-  return jacobi_smem(sg) > 0 ? pick_jacobi<true>(T, ppt, unroll) : pick_jacobi<false>(T, ppt, unroll);
+static JacobiKernel jacobi_kernel(int mode, int T, int ppt, int unroll) {
+  switch (mode) {
+    case kGradSmem: return pick_jacobi<kGradSmem>(T, ppt, unroll);
+    case kGradFlat: return pick_jacobi<kGradFlat>(T, ppt, unroll);
+    default: return pick_jacobi<kGradSpline>(T, ppt, unroll);
+  }
 }
 
-bool jacobi_variant_ok(int block, int ppt, int unroll) { return pick_jacobi<true>(block, ppt, unroll) != nullptr; }
+bool jacobi_variant_ok(int block, int ppt, int unroll) {
+  return pick_jacobi<kGradSpline>(block, ppt, unroll) != nullptr;
+}
 
-cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, int* blocks_per_sm, size_t* smem_out) {
-  JacobiKernel k = jacobi_kernel(sg, block, ppt, unroll);
+cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, bool spline, int* blocks_per_sm, size_t* smem_out) {
+  const int mode = grad_mode(sg, spline);
+  JacobiKernel k = jacobi_kernel(mode, block, ppt, unroll);
   if (!k) return cudaErrorInvalidValue;
-  const size_t smem = jacobi_smem(sg);
+  const size_t smem = jacobi_smem(mode, sg);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
@@ -494,7 +510,7 @@ cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, int* blocks_pe
 
 cudaError_t launch_jacobi(const JacobiArgs& a, int grid, int block, int ppt, int unroll, size_t smem,
                           cudaStream_t s) {
-  JacobiKernel k = jacobi_kernel(a.c.sg, block, ppt, unroll);
+  JacobiKernel k = jacobi_kernel(grad_mode(a.c.sg, a.grad_spline != 0), block, ppt, unroll);
   if (!k) return cudaErrorInvalidValue;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
