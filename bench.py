@@ -480,6 +480,43 @@ def bench_batched(args):
         dist.destroy_process_group()
 
 
+def bench_solve_shapes(args):
+    """k_jacobi alone on the 1M dam break at 10 fixed Jacobi iterations, for
+    each launch shape in --solve-shapes (threads,particles per thread,unroll):
+    CUDA events around the solve launch on the library's stream, median over
+    args.steps steps after 2 discarded ones.  One JSON line per shape."""
+    import torch
+
+    from warpsph_b200 import _lib
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+    from warpsph_b200.solver import IISPH
+
+    scene = preset_scene(PRESET)
+    dev = torch.device("cuda", 0)
+    steps = max(3, args.steps)
+    for shape in args.solve_shapes.split():
+        T, P, U = (int(v) for v in shape.split(","))
+        s = IISPH(stage_path=None, params=preset_params(PRESET, device=0, fixed_iters=10, warm_start="zero",
+                                                          jacobi_block=T, jacobi_ppt=P, jacobi_unroll=U), scene=scene)
+        st = torch.cuda.ExternalStream(s._lib.sph_stream(s._ctx), device=dev)
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(steps + 2)]
+        torch.cuda.synchronize()
+        for e in ev:
+            _lib.check(s._ctx, s._lib.sph_launch_phase(s._ctx, 0))
+            e[0].record(st)
+            _lib.check(s._ctx, s._lib.sph_launch_phase(s._ctx, 3))
+            e[1].record(st)
+        torch.cuda.synchronize()
+        t = sorted(e[0].elapsed_time(e[1]) for e in ev[2:])
+        h = s.stats_history(steps + 2)[-1]
+        s.close()
+        med = t[len(t) // 2]
+        byts = 10 * (100.0 * scene.n + 8.0 * h["n_ff_pairs"]) + 112.0 * scene.n
+        print(json.dumps({"solve_shape": [T, P, U], "ms": med, "us_per_iteration": med * 100.0,
+                          "GBps": byts / (med / 1e3) / 1e9, "iterations": h["iterations"]}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -489,6 +526,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true", help="only warm-up + K steps (for ncu captures)")
     ap.add_argument("--workload", choices=["dam_break_1m", "batched64"], default="dam_break_1m")
+    ap.add_argument("--solve-shapes", default="",
+                    help="time k_jacobi alone (10 fixed iterations) for these launch shapes, e.g. "
+                         "'256,1,4 256,1,2' (threads,particles per thread,unroll)")
     ap.add_argument("--warm", choices=["zero", "half", "mlp"], default="mlp",
                     help="warm start of the headline run: mlp = learned (default), zero = the "
                          "reference's p <- 0, half = 0.5 p_prev")
@@ -497,6 +537,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         bench_reference(args)
+    elif args.solve_shapes:
+        bench_solve_shapes(args)
     elif args.workload == "batched64":
         bench_batched(args)
     else:

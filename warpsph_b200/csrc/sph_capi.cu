@@ -950,11 +950,10 @@ int sph_set_pressure(SphCtx* ctx, const float* p, int64_t n) {
   if (!ctx || !p || n != ctx->n) return fail(ctx, SPH_E_INVALID, "pressure length must equal the fluid count");
   CK(cudaSetDevice(ctx->dev));
   if (n == 0) return SPH_OK;
-  std::vector<int> orig(n);
-  std::vector<float> ps(n);
-  CK(cudaMemcpy(orig.data(), ctx->orig_s, sizeof(int) * n, cudaMemcpyDeviceToHost));
-  for (int64_t k = 0; k < n; ++k) ps[k] = p[orig[k]];
-  CK(cudaMemcpy(ctx->p_s, ps.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  // one copy in original order, then a gather into the state's sorted order
+  CK(cudaMemcpyAsync(ctx->stage, p, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
+  CK(sph::launch_sort1(int(n), ctx->orig_s, ctx->stage, ctx->p_s, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   return SPH_OK;
 }
 
