@@ -480,6 +480,55 @@ def bench_batched(args):
         dist.destroy_process_group()
 
 
+def bench_pour(args):
+    """The pour onto a procedural obstacle (warpsph_b200.pour): the inlet
+    emits layers until 2,000,000 fluid particles have entered (untimed, device
+    appends between step batches), then K steps are timed with the emitter off
+    (CUDA events on the library's stream).  Prints its own JSON line."""
+    import torch
+
+    from warpsph_b200 import _lib, pour
+
+    dev = torch.device("cuda", 0)
+    sol, inlet = pour.make(warm_start=args.warm)
+    t0 = time.perf_counter()
+    emit_steps = pour.emit_until(sol, inlet)
+    emit_s = time.perf_counter() - t0
+    if args.warmup:
+        sol.steps(args.warmup)
+    _lib.check(sol._ctx, sol._lib.sph_prepare(sol._ctx))
+    st = torch.cuda.ExternalStream(sol._lib.sph_stream(sol._ctx), device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    e0.record(st)
+    _lib.check(sol._ctx, sol._lib.sph_launch_steps(sol._ctx, args.steps))
+    e1.record(st)
+    e1.synchronize()
+    clock = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    hist = sol.stats_history(args.steps)
+    flags = 0
+    for h in hist:
+        flags |= h["flags"]
+    if flags & (_lib.SPH_F_TIMEOUT | _lib.SPH_F_NONFINITE | _lib.SPH_F_FF_OVERFLOW | _lib.SPH_F_FB_OVERFLOW):
+        raise RuntimeError(f"step flags {flags:#x} in the timed region")
+    line = {"metric": "IISPH steps/s, 2M-particle pour onto a procedural obstacle", "value": args.steps / (ms / 1e3),
+            "unit": "steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"pour: {sol.n} fluid + {sol.boundary_n} boundary particles, 0.008 m, "
+                                   f"steps after emission ended", "warm_start": args.warm},
+            "particle_updates_per_s": sol.n * args.steps / (ms / 1e3),
+            "jacobi_iterations_mean": float(np.mean([h["iterations"] for h in hist])),
+            "n_ff_pairs_mean": float(np.mean([h["n_ff_pairs"] for h in hist])),
+            "v_max_max": float(max(h["v_max"] for h in hist)),
+            "emission": {"steps": emit_steps, "wall_s": emit_s, "sim_time": sol.sim_time},
+            "clocks": clock}
+    sol.close()
+    print(json.dumps(line), flush=True)
+
+
 def bench_solve_shapes(args):
     """k_jacobi alone on the 1M dam break at 10 fixed Jacobi iterations, for
     each launch shape in --solve-shapes (threads,particles per thread,unroll):
@@ -525,22 +574,27 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true", help="only warm-up + K steps (for ncu captures)")
-    ap.add_argument("--workload", choices=["dam_break_1m", "batched64"], default="dam_break_1m")
+    ap.add_argument("--workload", choices=["dam_break_1m", "batched64", "pour_2m"], default="dam_break_1m")
     ap.add_argument("--solve-shapes", default="",
                     help="time k_jacobi alone (10 fixed iterations) for these launch shapes, e.g. "
                          "'256,1,4 256,1,2' (threads,particles per thread,unroll)")
-    ap.add_argument("--warm", choices=["zero", "half", "mlp"], default="mlp",
-                    help="warm start of the headline run: mlp = learned (default), zero = the "
-                         "reference's p <- 0, half = 0.5 p_prev")
+    ap.add_argument("--warm", choices=["zero", "half", "mlp"], default=None,
+                    help="warm start of the headline run: mlp = learned (default for the dam break and "
+                         "the batch), zero = the reference's p <- 0 (default for the pour, whose splashes "
+                         "lie outside the network's dam-break training data), half = 0.5 p_prev")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.warm is None:
+        args.warm = "zero" if args.workload == "pour_2m" else "mlp"
     if args.impl == "reference":
         bench_reference(args)
     elif args.solve_shapes:
         bench_solve_shapes(args)
     elif args.workload == "batched64":
         bench_batched(args)
+    elif args.workload == "pour_2m":
+        bench_pour(args)
     else:
         bench_ours(args)
 

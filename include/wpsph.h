@@ -125,6 +125,16 @@ int sph_set_boundary(SphCtx* ctx, const float* xb3, const float* vb3, int64_t nb
 /* Fluid particles (IISPH.py:993-994) with velocities (NULL = zero). */
 int sph_set_fluid(SphCtx* ctx, const float* x3, const float* v3, int64_t n);
 
+/* Append `count` fluid particles (velocities NULL = zero, pressure 0) to the
+ * current state, keeping every existing particle's state; the new particles get
+ * original ids n .. n + count - 1.  For emitters (an inlet adding a layer of
+ * particles every few steps).  No counterpart in the reference, whose particle
+ * set is fixed at init_particles (IISPH.py:857-1000).  Single-scene contexts
+ * only.  The neighbour grid is not refitted: give params->domain_* to cover the
+ * region the emitted fluid will reach (particles outside the grid stay correct,
+ * in the clamped edge cells, but make those cells long). */
+int sph_add_fluid(SphCtx* ctx, const float* x3, const float* v3, int64_t count);
+
 /* ---- Batches of independent scenes ---------------------------------------
  * No counterpart in the reference (one scene per IISPH object).  All scenes
  * share the physical parameters and advance together: one sort, one build and

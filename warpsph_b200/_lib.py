@@ -102,6 +102,7 @@ SIGNATURES = {
     "sph_destroy": (None, [_P]),
     "sph_last_error": (ctypes.c_char_p, [_P]),
     "sph_set_tables": (ctypes.c_int, [_P, _P, ctypes.c_int32, _P, ctypes.c_int32]),
+    "sph_add_fluid": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64]),
     "sph_build_tables": (ctypes.c_int, [ctypes.POINTER(SphParams), _P, _P]),
     "sph_set_boundary": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64]),
     "sph_set_fluid": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64]),

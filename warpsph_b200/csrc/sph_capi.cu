@@ -939,11 +939,69 @@ int sph_set_fluid(SphCtx* ctx, const float* x3, const float* v3, int64_t n) {
     float* sv = ctx->stage + 3 * n;
     CK(cudaMemcpyAsync(sx, x3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
     if (v3) CK(cudaMemcpyAsync(sv, v3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
-    CK(sph::launch_pack_fluid(int(n), sx, v3 ? sv : nullptr, ctx->pos_s, ctx->vel_s, ctx->orig_s, ctx->p_s,
+    CK(sph::launch_pack_fluid(int(n), 0, sx, v3 ? sv : nullptr, ctx->pos_s, ctx->vel_s, ctx->orig_s, ctx->p_s,
                               ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
   }
   return SPH_OK;
+}
+
+int sph_add_fluid(SphCtx* ctx, const float* x3, const float* v3, int64_t count) {
+  if (!ctx || count < 0 || (count > 0 && !x3)) return fail(ctx, SPH_E_INVALID, "bad fluid arguments");
+  if (ctx->S != 1) return fail(ctx, SPH_E_INVALID, "sph_add_fluid takes single-scene contexts");
+  const int64_t n0 = ctx->n, n1 = n0 + count;
+  if (n1 > INT32_MAX / 64) return fail(ctx, SPH_E_INVALID, "too many fluid particles");
+  if (count == 0) return SPH_OK;
+  CK(cudaSetDevice(ctx->dev));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (n1 > ctx->n_cap || !ctx->pos_s) {
+    // grow by half at least, carrying the state (x, v, original ids, p) over
+    const int64_t cap = std::max<int64_t>(n1, ctx->n_cap + ctx->n_cap / 2);
+    float4 *tx = nullptr, *tv = nullptr;
+    int* to = nullptr;
+    float* tp = nullptr;
+    if (n0 > 0) {
+      CK(dalloc(tx, n0));
+      CK(dalloc(tv, n0));
+      CK(dalloc(to, n0));
+      CK(dalloc(tp, n0));
+      CK(cudaMemcpyAsync(tx, ctx->pos_s, sizeof(float4) * n0, cudaMemcpyDeviceToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(tv, ctx->vel_s, sizeof(float4) * n0, cudaMemcpyDeviceToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(to, ctx->orig_s, sizeof(int) * n0, cudaMemcpyDeviceToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(tp, ctx->p_s, sizeof(float) * n0, cudaMemcpyDeviceToDevice, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+    }
+    int rc = alloc_fluid(ctx, cap);
+    if (rc) return rc;
+    if (n0 > 0) {
+      CK(cudaMemcpyAsync(ctx->pos_s, tx, sizeof(float4) * n0, cudaMemcpyDeviceToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(ctx->vel_s, tv, sizeof(float4) * n0, cudaMemcpyDeviceToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(ctx->orig_s, to, sizeof(int) * n0, cudaMemcpyDeviceToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(ctx->p_s, tp, sizeof(float) * n0, cudaMemcpyDeviceToDevice, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      dfree(tx);
+      dfree(tv);
+      dfree(to);
+      dfree(tp);
+    }
+  }
+  float* sx = ctx->stage;
+  float* sv = ctx->stage + 3 * count;  // stage holds 7 floats per particle of capacity
+  CK(cudaMemcpyAsync(sx, x3, sizeof(float) * 3 * count, cudaMemcpyHostToDevice, ctx->stream));
+  if (v3) CK(cudaMemcpyAsync(sv, v3, sizeof(float) * 3 * count, cudaMemcpyHostToDevice, ctx->stream));
+  CK(sph::launch_pack_fluid(int(count), int(n0), sx, v3 ? sv : nullptr, ctx->pos_s, ctx->vel_s, ctx->orig_s,
+                            ctx->p_s, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->n = n1;
+  ctx->f_off = {0, n1};
+  ctx->graph_dirty = true;
+  if (!ctx->grid_valid) {
+    const int rc = set_grid(ctx, nullptr, 0);
+    if (rc < 0) return rc;
+    if (rc == 1) return sort_boundary(ctx);
+    return SPH_OK;
+  }
+  return upload_scene_table(ctx);  // the solve's chunks cover the new count
 }
 
 int sph_set_pressure(SphCtx* ctx, const float* p, int64_t n) {

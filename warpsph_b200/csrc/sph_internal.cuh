@@ -449,8 +449,8 @@ bool jacobi_variant_ok(int block, int ppt, int unroll);
 cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, bool spline, int* blocks_per_sm, size_t* smem);
 cudaError_t launch_jacobi(const JacobiArgs& a, int grid, int block, int ppt, int unroll, size_t smem,
                           cudaStream_t s);
-cudaError_t launch_pack_fluid(int n, const float* x3, const float* v3, float4* pos, float4* vel, int* orig,
-                              float* p, cudaStream_t s);
+cudaError_t launch_pack_fluid(int n, int base, const float* x3, const float* v3, float4* pos, float4* vel,
+                              int* orig, float* p, cudaStream_t s);
 cudaError_t launch_unsort4(int n, const int* orig, const float4* src, int component, float* out, cudaStream_t s);
 cudaError_t launch_unsort1(int n, const int* orig, const float* src, float* out, cudaStream_t s);
 cudaError_t launch_sort1(int n, const int* orig, const float* src, float* out, cudaStream_t s);

@@ -132,6 +132,21 @@ PRESETS = {
 }
 
 
+# Fluid poured from a 0.3 x 0.3 m inlet at 2 m/s onto a procedural obstacle
+# in a 2 m cube (scenes.pour_scene): 0.008 m spacing, dt = 4e-4 s, until 2M fluid.
+POUR = dict(diameter=0.008, domain=(2.0, 2.0, 2.0), layers=2, max_particles=2_000_000, seed=2, steps=1000)
+
+
+def pour_params(**kw) -> SolverParams:
+    d = POUR["diameter"] * (POUR["layers"] + 1)
+    lo = tuple(-d for _ in range(3))
+    hi = tuple(b + d for b in POUR["domain"])
+    base = dict(diameter=POUR["diameter"], gravity=9.81, w_table_size=1024, g_table_size=1024,
+                domain_min=lo, domain_max=hi)
+    base.update(kw)
+    return SolverParams(**base)
+
+
 def preset_params(name: str, **kw) -> SolverParams:
     cfg = PRESETS[name]
     base = dict(diameter=cfg["diameter"], gravity=9.81, w_table_size=1024, g_table_size=1024)

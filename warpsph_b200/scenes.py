@@ -102,15 +102,16 @@ def dam_break(fluid=(20, 20, 20), spacing=0.02, box=(1.0, 0.6, 0.4), jitter=1e-4
 
 
 def box_surface(lo, hi, spacing) -> np.ndarray:
-    """Particles on the six faces of the box [lo, hi]: every lattice point
-    lo + k * spacing (k >= 0, up to hi) with at least one coordinate on a face,
-    ordered x, y, z (z fastest)."""
+    """Particles on the six faces of the box [lo, hi]: the points of a lattice
+    with round((hi - lo) / spacing) + 1 (at least 2) evenly spaced planes per
+    axis, from lo to hi, that lie on a face; ordered x, y, z (z fastest)."""
     lo = np.asarray(lo, np.float64)
     hi = np.asarray(hi, np.float64)
-    n = [int(np.floor((h - l) / spacing + 1e-9)) + 1 for l, h in zip(lo, hi)]
+    n = [max(2, int(round((h - l) / spacing)) + 1) for l, h in zip(lo, hi)]
+    grids = [np.linspace(l, h, k) for l, h, k in zip(lo, hi, n)]
     ix, iy, iz = (a.ravel() for a in np.meshgrid(*[np.arange(k) for k in n], indexing="ij"))
     face = (ix == 0) | (ix == n[0] - 1) | (iy == 0) | (iy == n[1] - 1) | (iz == 0) | (iz == n[2] - 1)
-    pts = lo + spacing * np.stack([ix[face], iy[face], iz[face]], axis=1)
+    pts = np.stack([grids[0][ix[face]], grids[1][iy[face]], grids[2][iz[face]]], axis=1)
     return pts.astype(np.float32)
 
 
@@ -137,6 +138,120 @@ def add_obstacles(scene: Scene, obstacles) -> Scene:
     extra = [np.asarray(o, np.float32).reshape(-1, 3) for o in obstacles]
     bx = np.concatenate([scene.boundary_x] + extra).astype(np.float32)
     return Scene(scene.fluid_x, scene.fluid_v, bx, scene.boundary_hide_n, scene.box)
+
+
+def _inside_box(pts, lo, hi, margin):
+    return np.all((pts > np.asarray(lo) + margin) & (pts < np.asarray(hi) - margin), axis=1)
+
+
+def _inside_torus(pts, center, major, minor, axis, margin):
+    d = pts.astype(np.float64) - np.asarray(center, np.float64)
+    along = d[:, axis]
+    plane = np.delete(d, axis, axis=1)
+    ring = np.sqrt(np.sum(plane * plane, axis=1)) - major
+    return ring * ring + along * along < (minor - margin) ** 2
+
+
+def pour_obstacles(seed=2, spacing=0.008, boxes=6, tori=4, lo=(0.45, 0.25, 0.45), hi=(1.55, 1.2, 1.55),
+                   rmin=0.05, rmax=0.2):
+    """A seeded procedural obstacle: the union of `boxes` axis-aligned boxes
+    (half-extents uniform in [rmin, rmax] per axis) and `tori` tori (major
+    radius uniform in [rmin, rmax], tube radius 0.3-0.5 of it, axis x, y or z),
+    centres uniform in [lo, hi], surface-sampled at `spacing` (box_surface,
+    torus_surface).  Surface particles inside another shape are dropped, so
+    the particles sample the union's surface."""
+    rng = np.random.default_rng(seed)
+    shapes = []
+    for _ in range(boxes):
+        c = rng.uniform(lo, hi)
+        half = rng.uniform(rmin, rmax, size=3)
+        shapes.append(("box", c - half, c + half))
+    for _ in range(tori):
+        c = rng.uniform(lo, hi)
+        major = float(rng.uniform(rmin, rmax))
+        minor = max(2.0 * spacing, major * float(rng.uniform(0.3, 0.5)))
+        shapes.append(("torus", c, major, minor, int(rng.integers(0, 3))))
+    parts = []
+    for k, sh in enumerate(shapes):
+        pts = box_surface(sh[1], sh[2], spacing) if sh[0] == "box" else torus_surface(sh[1], sh[2], sh[3], spacing,
+                                                                                          axis=sh[4])
+        keep = np.ones(len(pts), bool)
+        for m, other in enumerate(shapes):
+            if m == k:
+                continue
+            if other[0] == "box":
+                keep &= ~_inside_box(pts, other[1], other[2], 0.5 * spacing)
+            else:
+                keep &= ~_inside_torus(pts, other[1], other[2], other[3], other[4], 0.5 * spacing)
+        parts.append(pts[keep])
+    return np.concatenate(parts).astype(np.float32), shapes
+
+
+class Inlet:
+    """A rectangular opening emitting fluid at a fixed speed along -y: a layer
+    of particles on a `spacing` lattice over the opening each time the previous
+    layer has moved one spacing on, i.e. every spacing / speed seconds, until
+    `max_particles` have been emitted.  Layer k leaves the opening at
+    t_k = k spacing / speed; at time t it is emitted (t - t_k) speed below the
+    opening with velocity speed along -y.  Seeded uniform jitter in
+    [-jitter, jitter] per coordinate."""
+
+    def __init__(self, center=(1.0, 1.8, 1.0), size=(0.3, 0.3), spacing=0.008, speed=2.0,
+                 max_particles=2_000_000, jitter=5e-5, seed=2):
+        nx, nz = int(round(size[0] / spacing)), int(round(size[1] / spacing))
+        ix, iz = (a.ravel() for a in np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij"))
+        self.offsets = np.stack([(ix - (nx - 1) / 2.0) * spacing, np.zeros(len(ix)), (iz - (nz - 1) / 2.0) * spacing],
+                                axis=1)
+        self.center = np.asarray(center, np.float64)
+        self.spacing, self.speed = float(spacing), float(speed)
+        self.period = self.spacing / self.speed
+        self.max_particles = int(max_particles)
+        self.jitter = float(jitter)
+        self.rng = np.random.default_rng(seed)
+        self.layers = 0
+        self.emitted = 0
+
+    @property
+    def layer_size(self) -> int:
+        return len(self.offsets)
+
+    @property
+    def done(self) -> bool:
+        return self.emitted >= self.max_particles
+
+    def due(self, t: float):
+        """Particles of every layer whose emission time is <= t and that has not
+        been emitted yet: (x, v), float32 arrays of shape (m, 3)."""
+        xs = []
+        while not self.done and self.layers * self.period <= t + 1e-12:
+            lag = t - self.layers * self.period
+            pts = self.center + self.offsets - np.array([0.0, lag * self.speed, 0.0])
+            if self.jitter > 0:
+                pts = pts + self.rng.uniform(-self.jitter, self.jitter, size=pts.shape)
+            pts = pts[: self.max_particles - self.emitted]
+            xs.append(pts)
+            self.layers += 1
+            self.emitted += len(pts)
+        if not xs:
+            return np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32)
+        x = np.concatenate(xs).astype(np.float32)
+        v = np.zeros_like(x)
+        v[:, 1] = -self.speed
+        return x, v
+
+
+def pour_scene(seed=2, spacing=0.008, domain=(2.0, 2.0, 2.0), layers=2):
+    """Fluid poured onto a procedural obstacle: a 2 x 2 x 2 m box walled by
+    `layers` boundary layers at `spacing`, the seeded obstacle union of
+    `pour_obstacles`, and the inlet's first layer as the initial fluid.
+    Returns (scene, inlet); feed inlet.due(sim_time) to IISPH.add_fluid."""
+    walls = box_boundary(domain, spacing, layers)
+    obstacle, _ = pour_obstacles(seed=seed, spacing=spacing)
+    inlet = Inlet(center=(domain[0] / 2, domain[1] * 0.9, domain[2] / 2), spacing=spacing, seed=seed)
+    x, v = inlet.due(0.0)
+    scene = Scene(fluid_x=x, fluid_v=v, boundary_x=walls.astype(np.float32), boundary_hide_n=len(walls),
+                  box=tuple(domain))
+    return add_obstacles(scene, [obstacle]), inlet
 
 
 def preset_scene(name: str) -> Scene:

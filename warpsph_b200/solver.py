@@ -158,6 +158,18 @@ class IISPH:
         self.n = len(x)
         _lib.check(self._ctx, self._lib.sph_set_fluid(self._ctx, _lib.ptr(x), _lib.ptr(v), self.n))
 
+    def add_fluid(self, x, v=None):
+        """Append fluid particles (e.g. an emitter's new layer) to the state on
+        the device.  Existing particles keep their state; new ones start with
+        p = 0 and take the next original ids.  No counterpart in the reference,
+        whose particle set is fixed at init_particles."""
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 3)
+        if len(x) == 0:
+            return
+        v = None if v is None else np.ascontiguousarray(v, dtype=np.float32).reshape(-1, 3)
+        _lib.check(self._ctx, self._lib.sph_add_fluid(self._ctx, _lib.ptr(x), _lib.ptr(v), len(x)))
+        self.n += len(x)
+
     def set_boundary_velocity(self, vb):
         """Boundary particle velocities (original order).  Re-uploads the
         boundary at its current positions, which recomputes psi there."""
