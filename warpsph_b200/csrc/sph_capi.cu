@@ -571,7 +571,8 @@ int enqueue_warm(SphCtx* ctx) {
     m.p_unit = float(ctx->P.rho0 * ctx->P.gravity * ctx->P.h);
     m.p0 = ctx->p_a;
     m.pos_q = ctx->pos_w;
-    CK(sph::launch_mlp_infer(m, ctx->sm_count, ctx->stream));
+    m.flags = &ctx->acc->flags;
+    CK(sph::launch_mlp_infer_tc(m, ctx->sm_count, ctx->stream));
   }
   return SPH_OK;
 }

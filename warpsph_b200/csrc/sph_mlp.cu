@@ -1,6 +1,8 @@
 // Learned pressure warm start: a per-particle MLP 10 -> 64 -> 64 -> 1 (ReLU),
-// BF16 operands on the tensor cores (mma.sync m16n8k16, FP32 accumulate),
-// with hand-written inference, training forward/backward and Adam kernels.
+// BF16 operands on the tensor cores with FP32 accumulation: the training
+// forward/backward here use warp-level mma.sync m16n8k16 tiles, the Adam
+// update runs on the CUDA cores, and the inference the step runs is the
+// tcgen05 kernel of sph_mlp_tc.cu (same BF16 rounding points).
 //
 // The network only proposes the Jacobi starting pressure p_0; the unchanged
 // relaxed-Jacobi loop (IISPH.py:1200-1296) still decides convergence, so a bad
@@ -139,51 +141,6 @@ __device__ __forceinline__ void feature_frag(const MlpSmem& s, const float* __re
     for (int h = 0; h < 2; ++h)
 #pragma unroll
       for (int q = 0; q < 4; ++q) xs[h][q] = bf16r(v[h][q]);
-  }
-}
-
-// ------------------------------------------------------------------ inference
-
-// The predicted pressure of every particle, written as the solve's first
-// iterate p_1 together with q_1 = p_1 / rho^2 (the .w of the particle's
-// position record) for the first Jacobi pass.  The network is residual on the previous step's pressure: with
-// u = asinh(p_prev / (rho0 g h)) (input 3, read here in float32, so the skip
-// path carries no bf16 rounding) the prediction is
-//   p_1 = sinh(max(u + min(y t_scale, kMaxRise), 0)) rho0 g h.
-// The rise over the previous pressure is bounded: the solve's stopping test
-// only counts compressed particles, so an over-predicted pressure (a network
-// extrapolating on an outlier such as a splash particle with a tiny a_ii) could
-// pass it after the minimum 2 iterations and kick the particle out of the
-// fluid.  Lower predictions only move the start toward p = 0.
-__global__ void __launch_bounds__(128) k_mlp_infer(MlpInferArgs a) {
-  __shared__ MlpSmem s;
-  load_weights(s, a.w);
-  __syncthreads();
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long tile = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); tile * 16 < a.n;
-       tile += warps) {
-    const long long r0 = tile * 16;
-    uint32_t a0, a1, a2, a3;
-    feature_frag(s, a.feat, r0, a.n, a0, a1, a2, a3);
-    Fwd f;
-    forward(s, a0, a1, a2, a3, f);
-    if (t == 0) {
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const long long i = r0 + g + 8 * h;
-        if (i < a.n) {
-          if (a.p0) {
-            const float u = __ldg(a.feat + i * kFeatures + 3);
-            const float p = sinhf(fmaxf(u + fminf(f.y[2 * h] * s.t_scale, kMaxRise), 0.f)) * a.p_unit;
-            const float rho = __ldg(a.rho + i);
-            a.p0[i] = p;
-            reinterpret_cast<float*>(a.pos_q + i)[3] = p / (rho * rho);
-          }
-          if (a.pred) a.pred[i] = f.y[2 * h];
-        }
-      }
-    }
   }
 }
 
@@ -473,15 +430,6 @@ cudaError_t launch_gather_rows(long long n, const int* idx, const float* feat, c
 
 cudaError_t launch_mlp_pack(const float* blob, MlpPacked* out, cudaStream_t s) {
   k_mlp_pack<<<8, 256, 0, s>>>(blob, out);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_mlp_infer(const MlpInferArgs& a, int sm_count, cudaStream_t s) {
-  if (a.n <= 0) return cudaSuccess;
-  const long long tiles = (a.n + 15) / 16;
-  long long blocks = (tiles + 3) / 4;
-  if (blocks > 8ll * sm_count) blocks = 8ll * sm_count;
-  k_mlp_infer<<<int(blocks), 128, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -55,6 +55,7 @@ struct MlpInferArgs {
   float* p0;              // out: initial pressure
   float4* pos_q;          // out: .w = p0 / rho^2 of each sorted position record
   float* pred;            // optional out: raw network output
+  int* flags;             // optional: SPH_F_TIMEOUT if a tensor-core wait ran out
 };
 
 struct MlpGradArgs {
@@ -78,7 +79,7 @@ struct MlpAdamArgs {
 
 size_t mlp_grad_smem();
 cudaError_t launch_mlp_pack(const float* blob, MlpPacked* out, cudaStream_t s);
-cudaError_t launch_mlp_infer(const MlpInferArgs& a, int sm_count, cudaStream_t s);
+cudaError_t launch_mlp_infer_tc(const MlpInferArgs& a, int sm_count, cudaStream_t s);  // tcgen05
 cudaError_t launch_mlp_grad(const MlpGradArgs& a, int nblocks, cudaStream_t s);
 cudaError_t launch_mlp_reduce_adam(const MlpAdamArgs& a, cudaStream_t s);
 cudaError_t launch_gather_rows(long long n, const int* idx, const float* feat, const float* target,

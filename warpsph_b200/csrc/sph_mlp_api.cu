@@ -158,12 +158,19 @@ int sph_mlp_eval(const float* blob, const float* feat, const float* target, int6
   CKR(cudaMemcpy(d_blob, blob, sizeof(float) * kBlobSize, cudaMemcpyHostToDevice));
   CKR(cudaMemcpy(d_feat, feat, sizeof(float) * n * kFeatures, cudaMemcpyHostToDevice));
   CKR(launch_mlp_pack(d_blob, d_w, nullptr));
+  int* d_flags;
+  CKR(B.alloc(d_flags, 1));
+  CKR(cudaMemset(d_flags, 0, sizeof(int)));
   MlpInferArgs ia{};
   ia.n = n;
   ia.w = d_w;
   ia.feat = d_feat;
   ia.pred = d_pred;
-  CKR(launch_mlp_infer(ia, sm, nullptr));
+  ia.flags = d_flags;
+  CKR(launch_mlp_infer_tc(ia, sm, nullptr));  // the step's inference kernel
+  int flags = 0;
+  CKR(cudaMemcpy(&flags, d_flags, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flags & SPH_F_TIMEOUT) return SPH_E_TIMEOUT;
   if (pred) CKR(cudaMemcpy(pred, d_pred, sizeof(float) * n, cudaMemcpyDeviceToHost));
   if (grad) {
     if (!target) return SPH_E_INVALID;
