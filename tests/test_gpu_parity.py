@@ -321,3 +321,64 @@ def test_nonfinite_input_raises():
         sol.step()
     assert e.value.code == SPH_E_NONFINITE
     sol.close()
+
+
+def test_no_boundary_free_fall_vs_oracle(oracle):
+    """A fluid block with no boundary particles at all (nb = 0): the build
+    skips the boundary grid and the solve has no boundary terms."""
+    from warpsph_b200.params import SolverParams
+    from warpsph_b200.scenes import Scene, dam_break
+
+    params = SolverParams(diameter=0.02, gravity=9.81, w_table_size=1024, g_table_size=1024)
+    block = dam_break(fluid=(10, 10, 10), spacing=0.02, box=(0.4, 0.4, 0.4), jitter=1e-4, layers=2, seed=11)
+    x = block.fluid_x.copy()
+    sc = Scene(x, np.zeros_like(x), np.zeros((0, 3), np.float32), 0, (0.4, 0.4, 0.4))
+    sol = _solver(params, sc)
+    ref = _oracle_step(oracle, params, x, np.zeros_like(x), np.zeros((0, 3), np.float32),
+                       np.zeros(0, np.float32), params.dt_max, 1 / params.dt_max)
+    sol.step()
+    nb = sol.get_neighbors()
+    assert csr_equal(nb["ff_off"], nb["ff_idx"], ref["ff_off"], ref["ff_idx"])
+    assert normrel(sol.rho.numpy(), ref["rho"]) < RTOL
+    assert abs(sol.last_stats["iterations"] - ref["iterations"]) <= 1
+    if sol.last_stats["iterations"] == ref["iterations"]:
+        assert normrel(sol.p.numpy(), ref["p"]) < RTOL
+        assert normrel(sol.v.numpy(), ref["v"]) < RTOL
+    sol.close()
+
+
+def test_coincident_particles_vs_oracle(oracle):
+    """Pairs of particles at exactly the same position: they are neighbours
+    (r = 0 < h), contribute W(0) to each other's density and, with a zero
+    direction, no gradient term (the reference's r < 1e-10 guard).  The
+    reference itself turns such a pair into NaN: predict_v_adv divides by
+    r^2 before multiplying the laplacian by VIS_MU = 0 (IISPH.py:273-278), and
+    the oracle, which restates it expression for expression, does the same.
+    The library drops that zero term (v_adv = v - g dt y exactly), so the
+    step stays finite."""
+    from warpsph_b200.params import SolverParams
+    from warpsph_b200.scenes import Scene, box_boundary, dam_break
+
+    params = SolverParams(diameter=0.02, gravity=9.81, w_table_size=1024, g_table_size=1024, fixed_iters=5)
+    block = dam_break(fluid=(8, 8, 8), spacing=0.02, box=(0.3, 0.3, 0.3), jitter=1e-4, layers=2, seed=12)
+    x = np.concatenate([block.fluid_x, block.fluid_x[::37]]).astype(np.float32)  # 14 exact duplicates
+    bx = box_boundary((0.3, 0.3, 0.3), 0.02, 2).astype(np.float32)
+    sc = Scene(x, np.zeros_like(x), bx, len(bx), (0.3, 0.3, 0.3))
+    sol = _solver(params, sc)
+    psi = sol.boundary_phi.numpy()
+    ref = _oracle_step(oracle, params, x, np.zeros_like(x), bx, psi, params.dt_max, 1 / params.dt_max,
+                       fixed_iters=5)
+    sol.step()
+    nb = sol.get_neighbors()
+    assert csr_equal(nb["ff_off"], nb["ff_idx"], ref["ff_off"], ref["ff_idx"])
+    assert normrel(sol.rho.numpy(), ref["rho"]) < RTOL  # density has no r^2 division
+    dup = np.arange(0, len(block.fluid_x), 37)
+    assert np.isnan(ref["v_adv"][dup]).all()             # the reference's 0 * inf
+    v_adv = sol.v_adv.numpy()
+    want = np.zeros_like(v_adv)
+    want[:, 1] = np.float32(-params.gravity) * np.float32(params.dt_max)
+    assert np.array_equal(v_adv, want)
+    for f in ("p", "v", "x"):
+        assert np.isfinite(getattr(sol, f).numpy()).all()
+    assert sol.last_stats["iterations"] == 5
+    sol.close()
