@@ -219,7 +219,9 @@ def bench_ours(args):
     K = args.steps
 
     def fresh(mode):
-        s = IISPH(stage_path=None, params=preset_params(PRESET, device=local, warm_start=mode), scene=scene)
+        # "mlp_continue": the learned start, and a step after a capped solve continues from its pressure
+        kw = dict(warm_start="mlp", warm_continue=True) if mode == "mlp_continue" else dict(warm_start=mode)
+        s = IISPH(stage_path=None, params=preset_params(PRESET, device=local, **kw), scene=scene)
         _lib.check(s._ctx, s._lib.sph_prepare(s._ctx))  # capture the step graph outside any timing
         return s
 
@@ -297,7 +299,7 @@ def bench_ours(args):
                                     "steps_above_tol": int((errs > 1e-3).sum())}}
 
     modes = {}
-    for mode in ("zero", "half", "mlp"):
+    for mode in ("zero", "half", "mlp", "mlp_continue"):
         if mode == headline:
             modes[mode] = mode_line(ms, hist)
             continue

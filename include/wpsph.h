@@ -83,7 +83,9 @@ typedef struct SphParams {
                             the boundary grid is rebuilt every step (IISPH.py:1415-1416); psi
                             keeps the values of sph_set_boundary, as the reference computes it
                             once (IISPH.py:811-821) */
-  int32_t reserved[1];
+  int32_t warm_continue;  /* 1 (SPH_WARM_MLP only): after a solve that stopped at the iteration
+                            cap, the next step of that scene starts from the capped solve's final
+                            pressure instead of the network's prediction */
 } SphParams;
 
 typedef struct SphStepStats { /* for a batch: max over scenes, dt and time of scene 0 */

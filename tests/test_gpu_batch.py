@@ -17,21 +17,27 @@ def _scenes():
             dam_break(fluid=(3, 3, 3), spacing=0.02, box=(0.2, 0.2, 0.2), jitter=1e-4, seed=4)]
 
 
-@pytest.mark.parametrize("warm", ["zero", "half"])
+@pytest.mark.parametrize("warm", ["zero", "half", "mlp_continue"])
 def test_batch_matches_individual_runs(warm):
+    """With "mlp_continue" the iteration cap is low, so some scenes' solves
+    stop at it and continue from their own pressure while the others start
+    from the network's prediction."""
     from warpsph_b200.batch import BatchIISPH
     from warpsph_b200.params import SolverParams
     from warpsph_b200.solver import IISPH
 
-    params = SolverParams(diameter=0.02, gravity=9.81, w_table_size=1024, g_table_size=1024, warm_start=warm)
+    kw = dict(warm_start="mlp", warm_continue=True, max_loop=8) if warm == "mlp_continue" else dict(warm_start=warm)
+    params = SolverParams(diameter=0.02, gravity=9.81, w_table_size=1024, g_table_size=1024, **kw)
     scenes = _scenes()
     b = BatchIISPH(scenes, params)
     steps = 40
     b.steps(steps)
     st = b.scene_stats()
+    capped = []
     for k, sc in enumerate(scenes):
         sol = IISPH(stage_path=None, params=params, scene=sc)
         sol.steps(steps)
+        capped.append(sum(h["iterations"] == params.max_loop + 1 for h in sol.stats_history(steps)))
         x, v, p = b.scene_fluid(k)
         assert np.array_equal(x, sol.x.numpy()), k
         assert np.array_equal(v, sol.v.numpy()), k
@@ -40,6 +46,8 @@ def test_batch_matches_individual_runs(warm):
         assert st["sim_time"][k] == sol.sim_time, k
         sol.close()
     b.close()
+    if warm == "mlp_continue":
+        assert sum(capped) > 0, capped
 
 
 def test_batch_scene_ranges_and_empty_scene():

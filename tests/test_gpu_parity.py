@@ -227,6 +227,41 @@ def test_warm_start_half_vs_oracle(oracle):
     sol2.close()
 
 
+def test_warm_continue_after_capped_solve_vs_oracle(oracle):
+    """Learned warm start with warm_continue: a solve that stopped at the
+    iteration cap hands its final pressure to the next step as that step's
+    first iterate, in place of the network's prediction.  The oracle's
+    "keep p" start (Ap of the given p, then Jacobi updates) with one update
+    fewer than the capped count is the same sequence of iterates."""
+    from warpsph_b200 import _lib
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+
+    max_loop = 3  # caps at 4 iterations: the dam break's first steps need ~100
+    scene = preset_scene("dam_break_8k")
+    params = preset_params("dam_break_8k", warm_start="mlp", warm_continue=True, max_loop=max_loop)
+    sol = _solver(params, scene)
+    sol.step()
+    assert sol.last_stats["iterations"] == max_loop + 1
+    assert sol.last_stats["flags"] & _lib.SPH_F_NOT_CONVERGED
+    x, v, p = sol.x.numpy(), sol.v.numpy(), sol.p.numpy()
+    psi = sol.boundary_phi.numpy()
+    dt = sol.dt
+    sol.step()
+    assert sol.last_stats["iterations"] == max_loop + 1
+    ref = _oracle_step(oracle, params, x, v, scene.boundary_x, psi, dt, 1.0 / dt, p=p, warm_start=2,
+                       fixed_iters=max_loop)
+    assert normrel(sol.p.numpy(), ref["p"]) < RTOL
+    assert normrel(sol.v.numpy(), ref["v"]) < RTOL
+    assert normrel(sol.x.numpy(), ref["x"]) < RTOL
+    # without warm_continue the second step starts from the network's prediction
+    plain = _solver(params.replace(warm_continue=False), scene)
+    plain.steps(2)
+    assert normrel(plain.p.numpy(), ref["p"]) > 100 * RTOL
+    sol.close()
+    plain.close()
+
+
 def test_deterministic_and_graph_equivalent():
     from warpsph_b200.params import preset_params
     from warpsph_b200.scenes import preset_scene

@@ -572,6 +572,12 @@ int enqueue_warm(SphCtx* ctx) {
     m.p0 = ctx->p_a;
     m.pos_q = ctx->pos_w;
     m.flags = &ctx->acc->flags;
+    if (ctx->P.warm_continue) {
+      // a scene whose last solve stopped at the cap continues from that solve
+      m.pprev = ctx->pprev_w;
+      m.restart = ctx->st->capped;
+      m.scenes = ctx->S > 1 ? ctx->d_scenes : nullptr;
+    }
     CK(sph::launch_mlp_infer_tc(m, ctx->sm_count, ctx->stream));
   }
   return SPH_OK;
@@ -773,6 +779,7 @@ int sph_create(const SphParams* params, SphCtx** out) {
       !(P.dt0 > 0) || !(P.dt_max > 0))
     return SPH_E_INVALID;
   if (!(P.vis_mu >= 0.0)) return SPH_E_INVALID;
+  if (P.warm_continue != 0 && P.warm_continue != 1) return SPH_E_INVALID;
   SphCtx* ctx = new SphCtx();
   ctx->P = P;
   if (ctx->P.timeout_ms <= 0) ctx->P.timeout_ms = 2000;

@@ -116,6 +116,7 @@ struct DevState {
   double dt64[kMaxScenes], inv_dt64[kMaxScenes];  // dt, 1/dt as the reference holds them
   double sim_time[kMaxScenes];
   float dt[kMaxScenes], inv_dt[kMaxScenes];       // what the kernels use (float32 arguments)
+  int capped[kMaxScenes];                         // 1: the last solve stopped at the iteration cap
   long long step_index;
 };
 

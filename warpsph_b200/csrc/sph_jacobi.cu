@@ -406,7 +406,9 @@ __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G) {
       for (int s = 0; s < a.nscenes; ++s) {
         const float vm = __uint_as_float(*(volatile unsigned int*)&acc->vmax_bits[s]);
         if (!isfinite(vm)) flags |= SPH_F_NONFINITE;
-        if (ok && acc->done[s] == 2 && c.fixed_iters <= 0) flags |= SPH_F_NOT_CONVERGED;
+        const bool capped = ok && acc->done[s] == 2 && c.fixed_iters <= 0;
+        if (capped) flags |= SPH_F_NOT_CONVERGED;
+        st->capped[s] = capped ? 1 : 0;
         double dt_next, inv_next;
         if (double(vm) >= double(float(a.inv_small_d))) {
           // numpy-2 float32 semantics of 0.4*DIAMETER / v_max (IISPH.py:1369)

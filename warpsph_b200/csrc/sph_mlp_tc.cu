@@ -291,7 +291,10 @@ __global__ void __launch_bounds__(kTile) k_mlp_infer_tc(MlpInferArgs a) {
     y += s.b3;
     if (live) {
       if (a.p0) {
-        const float p = sinhf(fmaxf(u_prev + fminf(y * s.t_scale, kMaxRise), 0.f)) * a.p_unit;
+        const int sc = a.scenes ? find_scene(a.scenes->fluid_off, a.scenes->nscenes, int(row)) : 0;
+        const float p = (a.restart && __ldg(a.restart + sc))
+                            ? __ldg(a.pprev + row)
+                            : sinhf(fmaxf(u_prev + fminf(y * s.t_scale, kMaxRise), 0.f)) * a.p_unit;
         const float rho = __ldg(a.rho + row);
         a.p0[row] = p;
         reinterpret_cast<float*>(a.pos_q + row)[3] = p / (rho * rho);

@@ -44,6 +44,7 @@ class SolverParams:
     jacobi_ppt: int = 0           # particles per solve thread (0 = 1)
     jacobi_unroll: int = 0        # solve neighbour-loop unroll (0 = 4)
     move_boundary: bool = False   # boundary moves with its velocities (DYNAMIC_SCENE, main.py:20)
+    warm_continue: bool = False   # "mlp": a step after a capped solve starts from that solve's pressure
     dt0: float | None = None      # None: TIME_STEP_MAX (IISPH.py:747)
     domain_min: tuple = (0.0, 0.0, 0.0)
     domain_max: tuple = (0.0, 0.0, 0.0)
@@ -112,6 +113,7 @@ class SolverParams:
         p.jacobi_ppt = self.jacobi_ppt
         p.jacobi_unroll = self.jacobi_unroll
         p.move_boundary = int(self.move_boundary)
+        p.warm_continue = int(self.warm_continue)
         return p
 
     @classmethod
