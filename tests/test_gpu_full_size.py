@@ -1,0 +1,85 @@
+"""The benchmark's own workload at full size: the 1,000,000-particle dam break
+(100 x 100 x 100 fluid lattice at 0.01 m, 206,464 boundary particles).
+
+One step from a moving state, 30 steps after the start, against the FP32 CPU
+oracle on the same inputs (the oracle finishes a full-size step in about a
+second on the host's threads), and properties that hold at any size: the
+neighbour relation is symmetric, the pair total the device counts equals the
+exported lists, and the solve's reported average density error is exactly
+what its exported terms give."""
+import numpy as np
+import pytest
+
+from tests.helpers import csr_equal, normrel
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-4
+FIXED = 4  # fixed Jacobi iterations: both sides stop after the same update
+
+
+@pytest.fixture(scope="module")
+def full_step(oracle):
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+    from warpsph_b200.solver import IISPH
+    from warpsph_b200.tables import kernel_tables
+
+    params = preset_params("dam_break_1m", keep_fb_lists=True)
+    scene = preset_scene("dam_break_1m")
+    run = IISPH(stage_path=None, params=params, scene=scene)
+    run.steps(30)
+    x, v, dt = run.x.numpy(), run.v.numpy(), run.dt
+    psi = run.boundary_phi.numpy()
+    run.close()
+
+    sol = IISPH(stage_path=None, params=params.replace(fixed_iters=FIXED), scene=scene)
+    sol.set_state(x, v)
+    sol.set_dt(dt, 1.0 / dt)
+    sol.step()
+    out = {"stats": dict(sol.last_stats), "nb": sol.get_neighbors(with_boundary=True),
+           "rho": sol.rho.numpy(), "rho_adv": sol.rho_adv.numpy(), "a_ii": sol.term_a_ii.numpy(),
+           "Ap": sol.term_Ap_i.numpy(), "p": sol.p.numpy(), "v": sol.v.numpy(), "x": sol.x.numpy()}
+    sol.close()
+
+    op = oracle.reference_params(diameter=params.diameter, gravity=params.gravity, w_size=params.w_table_size,
+                                 g_size=params.g_table_size)
+    ref = oracle.step(op, x, v, scene.boundary_x, None, psi, dt, 1.0 / dt, tables=kernel_tables(params),
+                      fixed_iters=FIXED)
+    return out, ref, params
+
+
+def test_full_size_step_vs_oracle(full_step):
+    out, ref, _ = full_step
+    assert out["stats"]["iterations"] == FIXED
+    assert csr_equal(out["nb"]["ff_off"], out["nb"]["ff_idx"], ref["ff_off"], ref["ff_idx"])
+    assert csr_equal(out["nb"]["fb_off"], out["nb"]["fb_idx"], ref["fb_off"], ref["fb_idx"])
+    for k in ("rho", "rho_adv", "a_ii", "p", "v"):
+        assert normrel(out[k], ref[k]) < RTOL, k
+    assert normrel(out["x"], ref["x"]) < 1e-6
+
+
+def test_full_size_neighbour_relation_symmetric(full_step):
+    out, _, _ = full_step
+    off = np.asarray(out["nb"]["ff_off"], np.int64)
+    idx = np.asarray(out["nb"]["ff_idx"], np.int64)
+    n = len(off) - 1
+    assert out["stats"]["n_ff_pairs"] == len(idx)
+    i = np.repeat(np.arange(n, dtype=np.int64), np.diff(off))
+    assert not np.any(i == idx)  # no particle lists itself
+    fwd = np.sort(i * n + idx)
+    bwd = np.sort(idx * n + i)
+    assert np.array_equal(fwd, bwd)
+
+
+def test_full_size_reported_error_matches_terms(full_step):
+    """update_rho_error + average_rho_error (IISPH.py:542-568, 1489-1494):
+    per particle in FP32, summed in FP64; only the summation order differs."""
+    out, _, params = full_step
+    rho0 = np.float32(params.rho0)
+    rp = (out["rho_adv"] + out["Ap"]).astype(np.float32)
+    hot = rp > rho0
+    err = np.abs(rp[hot] / rho0 - np.float32(1.0)).astype(np.float32)
+    want = float(np.sum(err.astype(np.float64)) / max(int(hot.sum()), 1))
+    assert abs(out["stats"]["avg_err"] - want) <= 1e-12 * max(want, 1e-30)
+    assert np.all(np.isfinite(out["x"])) and np.all(np.isfinite(out["v"])) and np.all(out["p"] >= 0)
