@@ -83,3 +83,70 @@ def test_full_size_reported_error_matches_terms(full_step):
     want = float(np.sum(err.astype(np.float64)) / max(int(hot.sum()), 1))
     assert abs(out["stats"]["avg_err"] - want) <= 1e-12 * max(want, 1e-30)
     assert np.all(np.isfinite(out["x"])) and np.all(np.isfinite(out["v"])) and np.all(out["p"] >= 0)
+
+
+def test_full_size_batch_of_64_matches_individual_runs():
+    """The batched workload at full size: 64 dam breaks of 5k-200k particles
+    (log-uniform, seeded) in one context with the learned warm start, against
+    the smallest, the median and the largest scene run alone, bit for bit."""
+    from warpsph_b200.batch import BatchIISPH
+    from warpsph_b200.params import SolverParams
+    from warpsph_b200.scenes import batched_scenes
+    from warpsph_b200.solver import IISPH
+
+    scenes = batched_scenes()
+    assert len(scenes) == 64
+    params = SolverParams(diameter=0.01, gravity=9.81, w_table_size=1024, g_table_size=1024, warm_start="mlp")
+    steps = 20
+    b = BatchIISPH(scenes, params)
+    b.steps(steps)
+    st = b.scene_stats()
+    order = np.argsort([s.n for s in scenes])
+    for k in (int(order[0]), int(order[len(order) // 2]), int(order[-1])):
+        sol = IISPH(stage_path=None, params=params, scene=scenes[k])
+        sol.steps(steps)
+        x, v, p = b.scene_fluid(k)
+        assert np.array_equal(x, sol.x.numpy()), k
+        assert np.array_equal(v, sol.v.numpy()), k
+        assert np.array_equal(p, sol.p.numpy()), k
+        assert st["iterations"][k] == sol.last_stats["iterations"], k
+        sol.close()
+    b.close()
+
+
+def test_full_size_pour_step_vs_oracle(oracle):
+    """The pour at full size: 2,000,000 particles emitted layer by layer onto
+    the seeded obstacle union (about 1M boundary particles), then one step of
+    the filled scene against the oracle: uneven cell occupancy, splashes and
+    particles resting on curved boundaries."""
+    from warpsph_b200 import _lib, pour
+    from warpsph_b200.params import POUR
+    from warpsph_b200.tables import kernel_tables
+
+    sol, inlet = pour.make(warm_start="zero", keep_fb_lists=True)
+    pour.emit_until(sol, inlet)
+    assert sol.n == POUR["max_particles"]
+    sol.steps(5)
+    hist = sol.stats_history(5)
+    assert not any(h["flags"] & (_lib.SPH_F_NONFINITE | _lib.SPH_F_TIMEOUT) for h in hist)
+    x, v, dt = sol.x.numpy(), sol.v.numpy(), sol.dt
+    psi = sol.boundary_phi.numpy()
+    bx = sol.boundary_x.numpy()
+    params = sol.params
+    sol.close()
+
+    one, _ = pour.make(warm_start="zero", keep_fb_lists=True, fixed_iters=FIXED)
+    one.set_state(x, v)
+    one.set_dt(dt, 1.0 / dt)
+    one.step()
+    nb = one.get_neighbors(with_boundary=True)
+    op = oracle.reference_params(diameter=params.diameter, gravity=params.gravity, w_size=params.w_table_size,
+                                 g_size=params.g_table_size)
+    ref = oracle.step(op, x, v, bx, None, psi, dt, 1.0 / dt, tables=kernel_tables(params), fixed_iters=FIXED)
+    assert one.last_stats["iterations"] == FIXED
+    assert csr_equal(nb["ff_off"], nb["ff_idx"], ref["ff_off"], ref["ff_idx"])
+    assert csr_equal(nb["fb_off"], nb["fb_idx"], ref["fb_off"], ref["fb_idx"])
+    for k, got in (("rho", one.rho), ("rho_adv", one.rho_adv), ("p", one.p), ("v", one.v)):
+        assert normrel(got.numpy(), ref[k]) < RTOL, k
+    assert normrel(one.x.numpy(), ref["x"]) < 1e-6
+    one.close()
