@@ -131,6 +131,17 @@ def collect(scenes, steps, per_step, params_for, seed=0, warm="half", skip=0):
     return np.concatenate(feats), np.concatenate(targets)
 
 
+def weighted_resample(feat, target, alpha, seed=0):
+    """Resample (feat, target) with replacement, pair k drawn with weight
+    1 + alpha * max(target_k, 0): the mean-squared loss then weighs the
+    pressurised interior, whose error sets how many Jacobi iterations a step
+    needs, above the free surface and splashes."""
+    t = np.asarray(target, np.float32)
+    w = 1.0 + alpha * np.maximum(t.astype(np.float64), 0.0)
+    pick = np.random.default_rng(seed).choice(len(t), size=len(t), replace=True, p=w / w.sum())
+    return np.ascontiguousarray(np.asarray(feat, np.float32)[pick]), np.ascontiguousarray(t[pick])
+
+
 def save(path, blob, **meta):
     np.savez_compressed(path, blob=np.asarray(blob, np.float32), **meta)
 
