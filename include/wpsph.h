@@ -85,7 +85,8 @@ typedef struct SphParams {
                             once (IISPH.py:811-821) */
   int32_t warm_continue;  /* 1 (SPH_WARM_MLP only): after a solve that stopped at the iteration
                             cap, the next step of that scene starts from the capped solve's final
-                            pressure instead of the network's prediction */
+                            pressure (or from sph_set_pressure's, if called in between) instead
+                            of the network's prediction; sph_set_fluid forgets the cap */
 } SphParams;
 
 typedef struct SphStepStats { /* for a batch: max over scenes, dt and time of scene 0 */

@@ -258,8 +258,20 @@ def test_warm_continue_after_capped_solve_vs_oracle(oracle):
     plain = _solver(params.replace(warm_continue=False), scene)
     plain.steps(2)
     assert normrel(plain.p.numpy(), ref["p"]) > 100 * RTOL
+    # a new state set after a capped solve starts from the prediction, as a
+    # context without that history does
+    x2, v2, dt2 = sol.x.numpy(), sol.v.numpy(), sol.dt
+    assert sol.last_stats["flags"] & _lib.SPH_F_NOT_CONVERGED
+    fresh = _solver(params, scene)
+    for s_ in (sol, fresh):
+        s_.set_state(x2, v2)
+        s_.set_dt(dt2, 1.0 / dt2)
+        s_.step()
+    assert np.array_equal(sol.p.numpy(), fresh.p.numpy())
+    assert np.array_equal(sol.x.numpy(), fresh.x.numpy())
     sol.close()
     plain.close()
+    fresh.close()
 
 
 def test_deterministic_and_graph_equivalent():

@@ -942,6 +942,8 @@ int sph_set_fluid(SphCtx* ctx, const float* x3, const float* v3, int64_t n) {
       if (rc) return rc;
     }
   }
+  // a new state: no solve of it has stopped at the cap yet (warm_continue)
+  CK(cudaMemsetAsync(ctx->st->capped, 0, sizeof(ctx->st->capped), ctx->stream));
   if (n > 0) {
     float* sx = ctx->stage;
     float* sv = ctx->stage + 3 * n;
