@@ -191,6 +191,13 @@ int sph_prepare(SphCtx* ctx);
  * Phases 0, 1 (or 0, 2, 3) in order make one step. */
 int sph_launch_phase(SphCtx* ctx, int32_t phase);
 
+/* Test hook for the solve's failure path (no reference counterpart): from the
+ * next step on, block `block` of the persistent solve skips its first
+ * grid-barrier arrival, so every block's bounded wait (timeout_ms) runs out;
+ * the step then returns SPH_E_TIMEOUT with the state, time and dt as they were
+ * before it.  -1 turns the hook off. */
+int sph_test_stall_barrier(SphCtx* ctx, int32_t block);
+
 /* IISPH.neighbor_search() (IISPH.py:1408-1482): cell sort + neighbour build +
  * density for the current state, without advancing time. */
 int sph_neighbor_search(SphCtx* ctx);

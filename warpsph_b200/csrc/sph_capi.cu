@@ -82,6 +82,7 @@ struct SphCtx {
   int blocks_per_sm = 0;
   size_t jac_smem = 0;
   int jac_block = 256, jac_ppt = 1, jac_unroll = 4;  // autotuner knobs of the solve
+  int stall_block = -1;                               // sph_test_stall_barrier
   int chunk = 256;                                    // particles per solve chunk
 
   DevState* st = nullptr;
@@ -625,6 +626,7 @@ int enqueue_jacobi(SphCtx* ctx) {
   j.start_iter = (ctx->P.warm_start == SPH_WARM_HALF) ? 0 : 1;
   j.grad_spline = ctx->g_spline ? 1 : 0;
   j.budget = (long long)ctx->P.timeout_ms * (long long)ctx->clock_khz;
+  j.stall_block = ctx->stall_block;
   j.dt_max = ctx->P.dt_max;
   j.cfl_len = ctx->P.cfl_len;
   j.inv_small_d = ctx->P.inv_small;
@@ -1090,6 +1092,15 @@ int sph_prepare(SphCtx* ctx) {
   rc = ensure_graph(ctx);
   if (rc) return rc;
   CK(cudaStreamSynchronize(ctx->stream));
+  return SPH_OK;
+}
+
+int sph_test_stall_barrier(SphCtx* ctx, int32_t block) {
+  if (!ctx || block < -1) return fail(ctx, SPH_E_INVALID, "block must be -1 or a block index");
+  if (ctx->stall_block != block) {
+    ctx->stall_block = block;
+    ctx->graph_dirty = true;
+  }
   return SPH_OK;
 }
 

@@ -303,8 +303,10 @@ __device__ inline int ld_volatile_int(const int* p) { return *(volatile const in
 // Grid-wide barrier for a cooperative (co-resident) launch.  Every wait is
 // bounded by `budget` SM cycles; on expiry it sets SPH_F_TIMEOUT and returns
 // false, and every later barrier returns false at once, so the kernel always
-// terminates and the host reads SPH_E_TIMEOUT.
-__device__ inline bool grid_barrier(StepAcc* acc, unsigned int nblocks, long long budget) {
+// terminates and the host reads SPH_E_TIMEOUT.  arrive = false (a test hook,
+// sph_test_stall_barrier) makes this block wait without arriving, so that
+// every block's wait runs out.
+__device__ inline bool grid_barrier(StepAcc* acc, unsigned int nblocks, long long budget, bool arrive = true) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -312,8 +314,8 @@ __device__ inline bool grid_barrier(StepAcc* acc, unsigned int nblocks, long lon
     if (ok) {
       unsigned int gen = ld_acquire(&acc->bar_gen);
       __threadfence();
-      unsigned int arrived = atomicAdd(&acc->bar_count, 1u);
-      if (arrived == nblocks - 1) {
+      unsigned int arrived = arrive ? atomicAdd(&acc->bar_count, 1u) : 0u;
+      if (arrive && arrived == nblocks - 1) {
         atomicExch(&acc->bar_count, 0u);
         __threadfence();
         atomicAdd(&acc->bar_gen, 1u);
@@ -421,6 +423,7 @@ struct JacobiArgs {
   int start_iter;          // 1: p_1 came from the build; 0: warm start, run pass 0
   int grad_spline;         // 1: the gradient table is the cubic spline's (closed form in the passes)
   long long budget;        // barrier spin budget in SM cycles
+  int stall_block;         // test hook: this block skips its first barrier arrival (-1: none)
   double dt_max, cfl_len, inv_small_d, eta_d;
 };
 

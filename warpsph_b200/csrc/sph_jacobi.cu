@@ -219,7 +219,10 @@ __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G) {
         pass_a<U>(i < r.y ? i : r.x, i < r.y, a, G, c.m * (dt * dt), pc);
       }
     }
-    if (!grid_barrier(acc, gridDim.x, a.budget)) { ok = false; break; }
+    if (!grid_barrier(acc, gridDim.x, a.budget, int(blockIdx.x) != a.stall_block)) {
+      ok = false;
+      break;
+    }
 
     // pass B: Ap, p_{k+1} and the density error.  A block's chunks visit the
     // scenes in non-decreasing order, so each scene is one contiguous run of
@@ -400,6 +403,10 @@ __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G) {
       __threadfence();
       DevState* st = a.st;
       int flags = *(volatile int*)&acc->flags;
+      // a wait ran out: no block ran the epilogue, so the state is still the
+      // step's input; time, dt and the statistics stay as they were and the
+      // host reports SPH_E_TIMEOUT (the step can be taken again)
+      if (flags & SPH_F_TIMEOUT) return;
       int iters = 0;
       double avg = 0.0, vmax_all = 0.0;
       const double dt_used0 = st->dt64[0];
