@@ -197,6 +197,12 @@ int sph_launch_phase(SphCtx* ctx, int32_t phase);
  * the step then returns SPH_E_TIMEOUT with the state, time and dt as they were
  * before it.  -1 turns the hook off. */
 int sph_test_stall_barrier(SphCtx* ctx, int32_t block);
+/* Test hook for the warm-start inference's failure path (no reference
+ * counterpart): with on = 1 the tensor-core inference issues no MMA, so its
+ * first bounded mbarrier wait runs out; the kernel frees its tensor memory and
+ * sets SPH_F_TIMEOUT, the solve then stops at its first barrier, and the step
+ * returns SPH_E_TIMEOUT with the state as it was.  0 turns the hook off. */
+int sph_test_withhold_mma(SphCtx* ctx, int32_t on);
 
 /* IISPH.neighbor_search() (IISPH.py:1408-1482): cell sort + neighbour build +
  * density for the current state, without advancing time. */

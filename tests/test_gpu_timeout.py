@@ -41,3 +41,36 @@ def test_barrier_timeout_reports_and_leaves_state():
     assert sol.sim_time > t0 and dt0 > 0
     sol.close()
     ref.close()
+
+
+def test_inference_wait_timeout_frees_tensor_memory():
+    """The learned warm start's tensor-core kernel with its MMAs withheld: its
+    bounded mbarrier wait runs out, it frees its tensor memory and flags the
+    step, the solve stops at its first barrier, and the step reports
+    SPH_E_TIMEOUT with the state untouched.  Afterwards inference allocates
+    tensor memory again and the retried step equals an undisturbed run's."""
+    from warpsph_b200 import _lib
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+    from warpsph_b200.solver import IISPH
+
+    params = preset_params("dam_break_8k", warm_start="mlp", timeout_ms=50)
+    scene = preset_scene("dam_break_8k")
+    sol = IISPH(stage_path=None, params=params, scene=scene)
+    ref = IISPH(stage_path=None, params=params, scene=scene)
+    sol.steps(3)
+    ref.steps(4)
+    x0, p0 = sol.x.numpy(), sol.p.numpy()
+
+    _lib.check(sol._ctx, sol._lib.sph_test_withhold_mma(sol._ctx, 1))
+    with pytest.raises(_lib.SphError) as err:
+        sol.step()
+    assert err.value.code == _lib.SPH_E_TIMEOUT
+    assert np.array_equal(sol.x.numpy(), x0) and np.array_equal(sol.p.numpy(), p0)
+
+    _lib.check(sol._ctx, sol._lib.sph_test_withhold_mma(sol._ctx, 0))
+    sol.step()
+    assert np.array_equal(sol.x.numpy(), ref.x.numpy())
+    assert np.array_equal(sol.p.numpy(), ref.p.numpy())
+    sol.close()
+    ref.close()

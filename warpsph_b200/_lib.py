@@ -113,6 +113,7 @@ SIGNATURES = {
     "sph_launch_steps": (ctypes.c_int, [_P, ctypes.c_int32]),
     "sph_launch_phase": (ctypes.c_int, [_P, ctypes.c_int32]),
     "sph_test_stall_barrier": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "sph_test_withhold_mma": (ctypes.c_int, [_P, ctypes.c_int32]),
     "sph_prepare": (ctypes.c_int, [_P]),
     "sph_neighbor_search": (ctypes.c_int, [_P]),
     "sph_get_fluid": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),

@@ -83,6 +83,7 @@ struct SphCtx {
   size_t jac_smem = 0;
   int jac_block = 256, jac_ppt = 1, jac_unroll = 4;  // autotuner knobs of the solve
   int stall_block = -1;                               // sph_test_stall_barrier
+  int withhold_mma = 0;                               // sph_test_withhold_mma
   int chunk = 256;                                    // particles per solve chunk
 
   DevState* st = nullptr;
@@ -573,6 +574,7 @@ int enqueue_warm(SphCtx* ctx) {
     m.p0 = ctx->p_a;
     m.pos_q = ctx->pos_w;
     m.flags = &ctx->acc->flags;
+    m.withhold_mma = ctx->withhold_mma;
     if (ctx->P.warm_continue) {
       // a scene whose last solve stopped at the cap continues from that solve
       m.pprev = ctx->pprev_w;
@@ -1099,6 +1101,15 @@ int sph_test_stall_barrier(SphCtx* ctx, int32_t block) {
   if (!ctx || block < -1) return fail(ctx, SPH_E_INVALID, "block must be -1 or a block index");
   if (ctx->stall_block != block) {
     ctx->stall_block = block;
+    ctx->graph_dirty = true;
+  }
+  return SPH_OK;
+}
+
+int sph_test_withhold_mma(SphCtx* ctx, int32_t on) {
+  if (!ctx || (on != 0 && on != 1)) return fail(ctx, SPH_E_INVALID, "on must be 0 or 1");
+  if (ctx->withhold_mma != on) {
+    ctx->withhold_mma = on;
     ctx->graph_dirty = true;
   }
   return SPH_OK;

@@ -56,6 +56,7 @@ struct MlpInferArgs {
   float4* pos_q;          // out: .w = p0 / rho^2 of each sorted position record
   float* pred;            // optional out: raw network output
   int* flags;             // optional: SPH_F_TIMEOUT if a tensor-core wait ran out
+  int withhold_mma;       // test hook: issue no MMA, so the first wait runs out
   const float* pprev;     // optional: previous-step pressure, sorted
   const int* restart;     // optional, per scene: 1 = start from pprev, not the prediction
   const SceneTable* scenes;  // scene of each row (null: one scene)

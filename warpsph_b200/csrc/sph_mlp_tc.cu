@@ -96,9 +96,11 @@ __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.a
 __device__ __forceinline__ void tc_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// Bounded wait for the mbarrier phase with parity `parity` to complete.
+// Bounded wait for the mbarrier phase with parity `parity` to complete.  An
+// MMA here completes in microseconds; 2^18 polls (each try_wait may suspend
+// the thread for a few microseconds) give up after about a second.
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (int it = 0; it < (1 << 22); ++it) {
+  for (int it = 0; it < (1 << 18); ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -232,8 +234,9 @@ __global__ void __launch_bounds__(kTile) k_mlp_infer_tc(MlpInferArgs a) {
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
-    // 2. layer 1 on the tensor cores
-    if (tid == 0) {
+    // 2. layer 1 on the tensor cores (the test hook withholds it: nothing is
+    // then in flight when the bounded wait below runs out)
+    if (tid == 0 && !a.withhold_mma) {
       mma_bf16_tc(d1, smem_desc(x_addr, 128, 16 * 16), smem_desc(w1_addr, 128, 16 * 16), idesc, 0);
       mma_commit(mbar);
     }
