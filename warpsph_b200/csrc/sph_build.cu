@@ -1,6 +1,6 @@
 // Neighbour build fused with everything of the step that depends only on
 // positions and velocities.  One thread per sorted fluid particle scans the
-// 3x3 rows of 3 x-adjacent cells (9 contiguous particle ranges) of the fluid
+// 3x3 rows of 5 x-adjacent half cells (9 contiguous particle ranges) of the fluid
 // grid and of the boundary grid once, and produces:
 //
 //   ELL list of fluid neighbours    count_same/store_same_neighbor (IISPH.py:52-104)
@@ -33,14 +33,14 @@
 namespace sph {
 
 // Phase 1 of the build for one particle: filter the candidates of the 3x3
-// rows of 3 x-adjacent cells with the exact float32 test and write the hits
+// rows of 5 x-adjacent half cells with the exact float32 test and write the hits
 // into the particle's ELL list.  Only a compare and a predicated store run per
 // candidate, so the warp stays converged; loads are issued four at a time.
 __device__ inline int filter_rows(const Grid& g, int base, int3 ci, const int* __restrict__ cell_start,
                                   const float4* __restrict__ pts, float4 xi, float r2_limit, int self, int* out,
                                   int K) {
   int cnt = 0;
-  const int x0 = max(ci.x - 1, 0), x1 = min(ci.x + 1, g.nx - 1);
+  const int x0 = max(ci.x - kXReach, 0), x1 = min(ci.x + kXReach, g.nx - 1);
   for (int cz = max(ci.z - 1, 0); cz <= min(ci.z + 1, g.nz - 1); ++cz) {
     for (int cy = max(ci.y - 1, 0); cy <= min(ci.y + 1, g.ny - 1); ++cy) {
       const int row = base + (cz * g.ny + cy) * g.nx;
@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(256) k_psi(PsiArgs a, float* psi) {
   const float4 xb = a.bpos[b];
   const int3 ci = cell_coord(g, xb.x, xb.y, xb.z);
   float rho = c.w0;
-  const int x0 = max(ci.x - 1, 0), x1 = min(ci.x + 1, g.nx - 1);
+  const int x0 = max(ci.x - kXReach, 0), x1 = min(ci.x + kXReach, g.nx - 1);
   for (int cz = max(ci.z - 1, 0); cz <= min(ci.z + 1, g.nz - 1); ++cz)
     for (int cy = max(ci.y - 1, 0); cy <= min(ci.y + 1, g.ny - 1); ++cy) {
       const int row = fr.base + (cz * g.ny + cy) * g.nx;

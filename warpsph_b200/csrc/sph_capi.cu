@@ -213,7 +213,8 @@ Grid fit_grid(const SphParams& P, const double* lo, const double* hi) {
   for (;;) {
     long long tot = 1;
     for (int a = 0; a < 3; ++a) {
-      dims[a] = std::max<long long>(1, (long long)std::ceil((hi[a] - lo[a] + 2 * pad) / cell) + 1);
+      const double w = a == 0 ? cell / sph::kXSplit : cell;
+      dims[a] = std::max<long long>(1, (long long)std::ceil((hi[a] - lo[a] + 2 * pad) / w) + 1);
       tot *= dims[a];
     }
     if (tot <= (1ll << 26)) break;
@@ -224,6 +225,7 @@ Grid fit_grid(const SphParams& P, const double* lo, const double* hi) {
   g.oy = float(lo[1] - pad);
   g.oz = float(lo[2] - pad);
   g.inv_cell = float(1.0 / cell);
+  g.inv_cell_x = float(sph::kXSplit / cell);
   g.nx = int(dims[0]);
   g.ny = int(dims[1]);
   g.nz = int(dims[2]);

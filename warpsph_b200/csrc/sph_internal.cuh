@@ -21,22 +21,28 @@ namespace sph {
 constexpr int kWarp = 32;
 constexpr int kFeatures = 10;  // learned warm-start inputs per particle
 
-// Uniform neighbour grid.  Cell size is slightly above h, so every neighbour
-// within h of a particle lies in the 3x3x3 cells around it even after float32
-// rounding of the cell coordinate.  Coordinates outside the grid are clamped to
-// the edge cells: clamping is monotone and 1-Lipschitz in cell space, so the
-// 27-cell search stays complete for particles that leave the domain.
+// Uniform neighbour grid.  Cell size is slightly above h (cell = 1.01 h or
+// coarser) in y and z; along x, the direction in which sorted rows run, cells
+// are cut in half (kXSplit), so a particle's neighbours within h lie in the
+// 5 half cells x-2..x+2 of the 3 x 3 rows around it: 2.5 cells wide instead
+// of 3, with the same 0.01 h margin for float32 rounding of the coordinate.
+// Coordinates outside the grid are clamped to the edge cells: clamping is
+// monotone and 1-Lipschitz in cell space, so the search stays complete for
+// particles that leave the domain.
+constexpr int kXSplit = 2;  // half cells along x
+constexpr int kXReach = 2;  // half cells searched on each side
 struct Grid {
   float ox, oy, oz;  // origin
-  float inv_cell;
-  int nx, ny, nz;
+  float inv_cell;    // 1 / cell (y, z)
+  float inv_cell_x;  // kXSplit / cell
+  int nx, ny, nz;    // nx counts half cells
   int ncells;
 };
 
 __host__ __device__ inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 __device__ inline int3 cell_coord(const Grid& g, float x, float y, float z) {
-  int cx = __float2int_rd((x - g.ox) * g.inv_cell);
+  int cx = __float2int_rd((x - g.ox) * g.inv_cell_x);
   int cy = __float2int_rd((y - g.oy) * g.inv_cell);
   int cz = __float2int_rd((z - g.oz) * g.inv_cell);
   return make_int3(clampi(cx, 0, g.nx - 1), clampi(cy, 0, g.ny - 1), clampi(cz, 0, g.nz - 1));

@@ -174,17 +174,19 @@ extern "C" int sph_boundary_psi_noalloc(const SphParams* params, const float* d_
   for (;;) {
     tot = 1;
     for (int a = 0; a < 3; ++a) {
-      dims[a] = std::max<long long>(1, (long long)std::ceil((hi[a] - lo[a] + 2 * pad) / cell) + 1);
+      const double w = a == 0 ? cell / kXSplit : cell;
+      dims[a] = std::max<long long>(1, (long long)std::ceil((hi[a] - lo[a] + 2 * pad) / w) + 1);
       tot *= dims[a];
     }
     if (tot <= kMaxCells) break;
-    cell *= 1.25;  // coarser cells keep the 27-cell search complete
+    cell *= 1.25;  // coarser cells keep the search complete
   }
   Grid g{};
   g.ox = float(lo[0] - pad);
   g.oy = float(lo[1] - pad);
   g.oz = float(lo[2] - pad);
   g.inv_cell = float(1.0 / cell);
+  g.inv_cell_x = float(kXSplit / cell);
   g.nx = int(dims[0]);
   g.ny = int(dims[1]);
   g.nz = int(dims[2]);

@@ -3,8 +3,9 @@
 // listed in IISPH.py:33-532).
 //
 // Order produced: ascending (cell index, original id).  The cell index runs x
-// fastest, so the three x-adjacent cells of a 3x3x3 neighbourhood are one
-// contiguous particle range.  Within a cell, particles are ordered by original
+// fastest (over half cells, Grid), so the x-adjacent cells of each of a
+// particle's 3x3 neighbour rows are one contiguous particle range.  Within a
+// cell, particles are ordered by original
 // id, which makes the sorted order a pure function of the positions (no
 // dependence on atomics or on the previous step's order).
 //
