@@ -136,13 +136,22 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
   return *reinterpret_cast<uint32_t*>(&v);
 }
 
+// BF16 pair (lo in the low half) of relu(lo), relu(hi), rounded to nearest
+// even in one conversion: for finite values relu commutes with the rounding
+// (it keeps signs), so this equals rounding fmaxf(v, 0).
+__device__ __forceinline__ uint32_t relu_pack2(float lo, float hi) {
+  uint32_t r;
+  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
+
 // relu(z + b) of 8 consecutive columns, rounded to BF16, as one 16-byte store.
 __device__ __forceinline__ void store_relu8(uint8_t* dst, const float* z, const float* b) {
   uint4 q;
-  q.x = pack2(fmaxf(z[0] + b[0], 0.f), fmaxf(z[1] + b[1], 0.f));
-  q.y = pack2(fmaxf(z[2] + b[2], 0.f), fmaxf(z[3] + b[3], 0.f));
-  q.z = pack2(fmaxf(z[4] + b[4], 0.f), fmaxf(z[5] + b[5], 0.f));
-  q.w = pack2(fmaxf(z[6] + b[6], 0.f), fmaxf(z[7] + b[7], 0.f));
+  q.x = relu_pack2(z[0] + b[0], z[1] + b[1]);
+  q.y = relu_pack2(z[2] + b[2], z[3] + b[3]);
+  q.z = relu_pack2(z[4] + b[4], z[5] + b[5]);
+  q.w = relu_pack2(z[6] + b[6], z[7] + b[7]);
   *reinterpret_cast<uint4*>(dst) = q;
 }
 
@@ -285,9 +294,11 @@ __global__ void __launch_bounds__(kTile) k_mlp_infer_tc(MlpInferArgs a) {
       for (int half = 0; half < 2; ++half) {
         tmem_ld32(d2 + lane_row + uint32_t(32 * half), z);
 #pragma unroll
-        for (int k = 0; k < 32; ++k) {
-          const float h = __bfloat162float(__float2bfloat16_rn(fmaxf(z[k] + s.b2[32 * half + k], 0.f)));
-          y = fmaf(h, s.w3[32 * half + k], y);
+        for (int k = 0; k < 32; k += 2) {
+          // relu + BF16 rounding of two columns at once, then back to FP32
+          const uint32_t hp = relu_pack2(z[k] + s.b2[32 * half + k], z[k + 1] + s.b2[32 * half + k + 1]);
+          y = fmaf(__uint_as_float(hp << 16), s.w3[32 * half + k], y);
+          y = fmaf(__uint_as_float(hp & 0xffff0000u), s.w3[32 * half + k + 1], y);
         }
       }
     }
