@@ -517,6 +517,7 @@ sph::BuildArgs build_args(SphCtx* ctx) {
   b.c = ctx->c;
   b.w_table = ctx->d_w;
   b.g_table = ctx->d_g;
+  b.spline = ctx->g_spline ? 1 : 0;
   b.pos = ctx->pos_w;
   b.vel = ctx->vel_w;
   b.pprev = ctx->pprev_w;

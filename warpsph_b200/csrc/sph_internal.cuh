@@ -365,6 +365,7 @@ struct SortArgs {
 
 struct BuildArgs {
   int n, nb;
+  int spline;              // 1: the gradient table is the cubic spline's own (closed form in the build)
   Grid grid;
   const SceneTable* scenes;
   Consts c;
