@@ -41,7 +41,15 @@ KERNELS_PER_STEP = 8
 
 
 def kernels_per_step(warm: str) -> int:
-    return KERNELS_PER_STEP + (1 if warm == "mlp" else 0)
+    return KERNELS_PER_STEP + (1 if warm.startswith("mlp") else 0)
+
+
+def warm_kwargs(mode: str) -> dict:
+    """SolverParams of a warm-start mode; "mlp_continue" is the learned start
+    that, after a solve stopped at the iteration cap, continues from it."""
+    if mode == "mlp_continue":
+        return dict(warm_start="mlp", warm_continue=True)
+    return dict(warm_start=mode)
 
 
 def _peaks():
@@ -219,9 +227,7 @@ def bench_ours(args):
     K = args.steps
 
     def fresh(mode):
-        # "mlp_continue": the learned start, and a step after a capped solve continues from its pressure
-        kw = dict(warm_start="mlp", warm_continue=True) if mode == "mlp_continue" else dict(warm_start=mode)
-        s = IISPH(stage_path=None, params=preset_params(PRESET, device=local, **kw), scene=scene)
+        s = IISPH(stage_path=None, params=preset_params(PRESET, device=local, **warm_kwargs(mode)), scene=scene)
         _lib.check(s._ctx, s._lib.sph_prepare(s._ctx))  # capture the step graph outside any timing
         return s
 
@@ -426,7 +432,7 @@ def bench_batched(args):
     scenes = [all_scenes[k] for k in mine]
     n = sum(s.n for s in scenes)
     params = SolverParams(diameter=0.01, gravity=9.81, w_table_size=1024, g_table_size=1024,
-                          warm_start=args.warm, device=local)
+                          device=local, **warm_kwargs(args.warm))
     tuned = at.autotune(scenes, params, warm=10, steps=10)
     tp = at.apply(params, tuned)
     K = args.steps
@@ -498,7 +504,7 @@ def bench_pour(args):
     from warpsph_b200 import _lib, pour
 
     dev = torch.device("cuda", 0)
-    sol, inlet = pour.make(warm_start=args.warm)
+    sol, inlet = pour.make(**warm_kwargs(args.warm))
     t0 = time.perf_counter()
     emit_steps = pour.emit_until(sol, inlet)
     emit_s = time.perf_counter() - t0
@@ -586,15 +592,16 @@ def main():
     ap.add_argument("--solve-shapes", default="",
                     help="time k_jacobi alone (10 fixed iterations) for these launch shapes, e.g. "
                          "'256,1,4 256,1,2' (threads,particles per thread,unroll)")
-    ap.add_argument("--warm", choices=["zero", "half", "mlp"], default=None,
-                    help="warm start of the headline run: mlp = learned (default for the dam break and "
-                         "the batch), zero = the reference's p <- 0 (default for the pour, whose splashes "
-                         "lie outside the network's dam-break training data), half = 0.5 p_prev")
+    ap.add_argument("--warm", choices=["zero", "half", "mlp", "mlp_continue"], default=None,
+                    help="warm start of the headline run: mlp_continue = learned, continuing from a solve "
+                         "that stopped at the iteration cap (default for the dam break), mlp = learned "
+                         "(default for the batch), zero = the reference's p <- 0 (default for the pour, "
+                         "whose splashes lie outside the network's dam-break training data), half = 0.5 p_prev")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.warm is None:
-        args.warm = "zero" if args.workload == "pour_2m" else "mlp"
+        args.warm = {"pour_2m": "zero", "batched64": "mlp"}.get(args.workload, "mlp_continue")
     if args.impl == "reference":
         bench_reference(args)
     elif args.solve_shapes:
