@@ -481,7 +481,7 @@ def bench_batched(args):
                 "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic",
                 "config": {"workload": f"64 dam breaks, {n_all} fluid particles in total, steps [0, {K})",
-                           "warm_start": params.warm_start, "parallelism": f"scenes sharded over {world}"},
+                           "warm_start": args.warm, "parallelism": f"scenes sharded over {world}"},
                 "particle_updates_per_s": n_all * K / (ms / 1000.0),
                 "sequential_contexts_steps_per_s": K / (seq_ms / 1000.0),
                 "batch_speedup": seq_ms / ms, "autotuned_rank0": {k: v for k, v in tuned.items() if k != "trials"},
