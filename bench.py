@@ -153,10 +153,10 @@ def run_cpu_reference(budget_s: float, max_steps: int, nthreads: int = 0):
     psi = oracle.boundary_psi(op, scene.boundary_x, tables=tabs, nthreads=nt)
     x0, v0, dt0 = scene.fluid_x.copy(), scene.fluid_v.copy(), params.dt_max
 
-    def one(x, v, dt, fixed=-1):
+    def one(x, v, dt, fixed=-1, threads=None):
         t0 = time.perf_counter()
         r = oracle.step(op, x, v, scene.boundary_x, None, psi, dt, 1.0 / dt, tables=tabs, export=False,
-                        nthreads=nt, fixed_iters=fixed)
+                        nthreads=threads or nt, fixed_iters=fixed)
         return time.perf_counter() - t0, r
 
     t2, _ = one(x0, v0, dt0, fixed=2)
@@ -166,6 +166,9 @@ def run_cpu_reference(budget_s: float, max_steps: int, nthreads: int = 0):
     K = max(1, max_steps)
     iters_ref = ref_iterations(K)
     value = K / (K * t_base + iters_ref * t_iter)
+
+    # the same 2-iteration step on one thread: the scaling of the port itself
+    t2_one, _ = one(x0, v0, dt0, fixed=2, threads=1)
 
     x, v, dt = x0, v0, dt0
     steps, t_total, iters = 0, 0.0, []
@@ -181,6 +184,7 @@ def run_cpu_reference(budget_s: float, max_steps: int, nthreads: int = 0):
                        f"initial state (steps with 2 and 12 fixed iterations); value = steps/s of steps [0, {K}) "
                        f"at the reference algorithm's {iters_ref:.0f} iterations for that range"),
             "ms_per_iteration": t_iter * 1e3, "ms_step_base": t_base * 1e3,
+            "one_thread": {"ms_step_2_iterations": t2_one * 1e3, "threads_speedup": t2_one / t2},
             "first_steps": {"steps": steps, "steps_per_s": steps / t_total, "iterations": iters}}
 
 
