@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -138,6 +139,17 @@ struct Ctx {
   }
 };
 
+// Per-pair storage (hundreds of MB at 1M particles) left uninitialised: every
+// element is written by a parallel loop before it is read, so its pages are
+// first touched by the threads that use them instead of being zeroed serially.
+template <typename T>
+struct Uninit {
+  std::unique_ptr<T[]> p;
+  explicit Uninit(size_t n) : p(new T[n > 0 ? n : 1]) {}
+  T& operator[](size_t i) { return p[i]; }
+  const T& operator[](size_t i) const { return p[i]; }
+};
+
 // Exact-distance neighbour sets on a uniform grid of cell size slightly above h.
 // N(i) = { j : |x_i - x_j| < h } (minus j = i when same == true), j ascending.
 // This restates the filtered hash_grid_query loops of IISPH.py:70-72 (ff),
@@ -175,12 +187,11 @@ void neighbours(const R* xq, int64_t nq, const R* xs, int64_t ns, R h, bool same
     std::vector<int64_t> fill(start.begin(), start.end() - 1);
     for (int64_t i = 0; i < ns; ++i) sorted[fill[key[i]]++] = int32_t(i);
   }
-  std::vector<std::vector<int32_t>> lists(nq);
-#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
-  for (int64_t i = 0; i < nq; ++i) {
+  // Two passes over the same candidates, count then fill, into one flat array
+  // (no per-particle allocations); each segment is then sorted ascending.
+  auto visit = [&](int64_t i, auto&& hit) {
     V3<R> xi{xq[3 * i], xq[3 * i + 1], xq[3 * i + 2]};
     int64_t c[3] = {coord(xi.x, 0), coord(xi.y, 1), coord(xi.z, 2)};
-    std::vector<int32_t>& L = lists[i];
     for (int64_t cz = std::max<int64_t>(c[2] - 1, 0); cz <= std::min(c[2] + 1, dim[2] - 1); ++cz)
       for (int64_t cy = std::max<int64_t>(c[1] - 1, 0); cy <= std::min(c[1] + 1, dim[1] - 1); ++cy)
         for (int64_t cx = std::max<int64_t>(c[0] - 1, 0); cx <= std::min(c[0] + 1, dim[0] - 1); ++cx) {
@@ -189,15 +200,24 @@ void neighbours(const R* xq, int64_t nq, const R* xs, int64_t ns, R h, bool same
             int32_t j = sorted[t];
             V3<R> xj{xs[3 * j], xs[3 * j + 1], xs[3 * j + 2]};
             R distance = length(xi - xj);
-            if (distance < h && !(same && j == i)) L.push_back(j);
+            if (distance < h && !(same && j == i)) hit(j);
           }
         }
-    std::sort(L.begin(), L.end());
+  };
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
+  for (int64_t i = 0; i < nq; ++i) {
+    int64_t n = 0;
+    visit(i, [&](int32_t) { ++n; });
+    off[i + 1] = n;
   }
-  for (int64_t i = 0; i < nq; ++i) off[i + 1] = off[i] + int64_t(lists[i].size());
+  for (int64_t i = 0; i < nq; ++i) off[i + 1] += off[i];
   idx.resize(off[nq]);
-#pragma omp parallel for schedule(static) num_threads(nthreads)
-  for (int64_t i = 0; i < nq; ++i) std::copy(lists[i].begin(), lists[i].end(), idx.begin() + off[i]);
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
+  for (int64_t i = 0; i < nq; ++i) {
+    int64_t w = off[i];
+    visit(i, [&](int32_t j) { idx[w++] = j; });
+    std::sort(idx.begin() + off[i], idx.begin() + off[i + 1]);
+  }
 }
 
 template <typename R>
@@ -270,7 +290,7 @@ int step(const OracleParams* P, OracleStep* S) {
   S->n_ff_pairs = Pff;
   S->n_fb_pairs = Pfb;
   // stored distances (IISPH.py:100-103, 159-162)
-  std::vector<R> ffd(Pff), fbd(Pfb);
+  Uninit<R> ffd(Pff), fbd(Pfb);
 #pragma omp parallel for schedule(static) num_threads(nt)
   for (int64_t i = 0; i < n; ++i) {
     V3<R> xi = ld3(x, i);
@@ -279,7 +299,8 @@ int step(const OracleParams* P, OracleStep* S) {
   }
 
   std::vector<R> rho(n), rho_adv(n), a_ii(n), Ap(n);
-  std::vector<V3<R>> v_adv(n), d_ii(n), s(n), d_ij(Pff), d_ji(Pff);
+  std::vector<V3<R>> v_adv(n), d_ii(n), s(n);
+  Uninit<V3<R>> d_ij(Pff), d_ji(Pff);
 
   // init_pressure (IISPH.py:166-174)
   if (P->warm_start == 0) std::fill(p, p + n, R(0));
