@@ -128,6 +128,16 @@ int sph_set_boundary(SphCtx* ctx, const float* xb3, const float* vb3, int64_t nb
 /* Fluid particles (IISPH.py:993-994) with velocities (NULL = zero). */
 int sph_set_fluid(SphCtx* ctx, const float* x3, const float* v3, int64_t n);
 
+/* Replace positions, velocities and pressures (original order) of the current
+ * fluid particles, keeping everything else the solver carries from step to
+ * step: dt, simulated time, the neighbour grid and the warm_continue cap flags
+ * (sph_set_fluid starts a new state and forgets them).  For callers that keep
+ * the state in host memory between steps (a checkpoint round trip, a coupled
+ * host-side code): stepping on after sph_get_fluid + sph_update_fluid gives
+ * the same result as stepping on directly.  n must equal the fluid count.
+ * No counterpart in the reference, whose state lives in Warp arrays. */
+int sph_update_fluid(SphCtx* ctx, const float* x3, const float* v3, const float* p, int64_t n);
+
 /* Append `count` fluid particles (velocities NULL = zero, pressure 0) to the
  * current state, keeping every existing particle's state; the new particles get
  * original ids n .. n + count - 1.  For emitters (an inlet adding a layer of
@@ -224,12 +234,33 @@ int sph_get_neighbors(SphCtx* ctx, int64_t* ff_off, int32_t* ff_idx, int64_t ff_
 int sph_get_stats(SphCtx* ctx, SphStepStats* out);
 /* Override dt / 1/dt for the next step (the reference's self.dt, self.inv_dt). */
 int sph_set_dt(SphCtx* ctx, double dt, double inv_dt);
+/* Solid sampling of a closed triangle mesh (scene generation): replaces the
+ * reference's model sampler (wp_sph/solver/model.py:14-60, `_sample_points` +
+ * `load_model`), used by init_particles for mesh scenes (IISPH.py:952-989).
+ * The caller passes the mesh (nv vertices, FP64 xyz; nt triangles, vertex
+ * indices) and the lattice axes xs, ys, zs (strictly ascending; the reference
+ * takes np.arange(lo, hi, spacing) over the mesh bounds); the library writes,
+ * in lattice order (x slowest, z fastest), every lattice point inside the
+ * mesh, transformed as p @ rot + pos (rot9 row-major 3 x 3, as numpy's
+ * `points @ rot`), as float32 xyz into out3 (cap points) and the number of
+ * such points into *count.  Inside means an odd number of crossings of the
+ * ray from the point along +x strictly beyond it (each crossing of a closed
+ * mesh counted once, also through shared edges and vertices).  A point on a
+ * face normal to x is inside on a face where +x enters the solid and outside
+ * on one where it leaves; elsewhere on the surface rounding decides.
+ * Returns SPH_E_TOO_LARGE (with *count set) if cap is too small,
+ * SPH_E_CAPACITY if one lattice line crosses the mesh more than 1024 times. */
+int sph_sample_solid(const double* verts3, int64_t nv, const int32_t* tris3, int64_t nt, const double* xs,
+                     int32_t nx, const double* ys, int32_t ny, const double* zs, int32_t nz, const double* rot9,
+                     const double* pos3, float* out3, int64_t cap, int64_t* count, int32_t device);
+
 /* Boundary volumes psi for callers that must not allocate device memory.
  * No counterpart in the reference: the reference always runs inside Warp,
  * which allocates freely.  This is for callers that cannot call cudaMalloc —
- * e.g. a host framework whose memory pool owns the device, code running while
- * a graph is captured in a mode that rejects allocations, or real-time code
- * that must not allocate after start-up.  The caller passes device pointers:
+ * e.g. a host framework whose memory pool owns the device and forbids
+ * allocations behind its back, or real-time code that must not allocate after
+ * start-up because an allocation can block or fail at any time.  The caller
+ * passes device pointers:
  * d_xb3 (nb x 3 floats, boundary positions), d_w_table (params->w_table_size
  * floats, the W table) and d_psi (nb floats, output in input order); it gets
  * the same psi as sph_set_boundary computes.  The library allocates nothing:
@@ -239,11 +270,14 @@ int sph_set_dt(SphCtx* ctx, double dt, double inv_dt);
  * most SPH_NOALLOC_MAX_CELLS grid cells (a coarser grid is chosen beyond that).
  * Runs on the calling thread's current device, on `stream` (a cudaStream_t,
  * NULL = default stream).  The first call on each device looks up the
- * scratch address (cudaGetSymbolAddress): make that first call before any
- * stream capture.  The call may synchronise `stream` (it reads the table's
- * first entry, and the grid extent when params->domain_* is empty); the psi
- * output is complete when `stream` is next synchronised.  All calls share the
- * scratch: calls whose GPU work overlaps (other streams or threads) race. */
+ * scratch's device address (cudaGetSymbolAddress) and keeps it: do not use
+ * this entry point on a device after cudaDeviceReset.  When params->domain_*
+ * is empty the call reads the points' bounding box back to the host and so
+ * synchronises `stream`; with a domain it only enqueues work (domain bounds
+ * must be finite, else SPH_E_INVALID).  The psi output is complete when
+ * `stream` is next synchronised.  All calls share the scratch, which keeps
+ * the last call's contents: calls whose GPU work overlaps (other streams or
+ * threads) race. */
 #define SPH_NOALLOC_MAX_BOUNDARY 262144
 #define SPH_NOALLOC_MAX_CELLS 1048576
 int sph_boundary_psi_noalloc(const SphParams* params, const float* d_xb3, int64_t nb, const float* d_w_table,
@@ -291,6 +325,13 @@ int sph_set_record_features(SphCtx* ctx, int32_t on);
 /* After a step: per fluid particle (original order) its SPH_MLP_FEATURES inputs
  * and the training target asinh(p / (rho0 g h)) of its converged pressure. */
 int sph_get_features(SphCtx* ctx, float* feat, float* target);
+/* After a step with sph_set_record_features(ctx, 1): per fluid particle
+ * (original order) the pressure the step's Jacobi solve started from — the
+ * iterate that replaces init_pressure (IISPH.py:166-174): the first update_p
+ * from p = 0 with SPH_WARM_ZERO, 0.5 p_prev with SPH_WARM_HALF (before the
+ * extra Ap_0 pass), and with SPH_WARM_MLP the network's prediction or, after
+ * a capped solve with warm_continue, that solve's final pressure. */
+int sph_get_solve_start(SphCtx* ctx, float* p);
 /* Train in place: Adam on mean squared error over shuffled minibatches, on the
  * GPU with the library's own forward/backward kernels.  blob supplies mu, sd,
  * t_scale and the initial weights; epoch_loss (epochs floats) may be NULL. */

@@ -81,3 +81,85 @@ def loss_and_grad(blob, feat, target):
     dW1 = f["xb"].T @ dz1b
     grad = np.concatenate([dW1.ravel(), db1, dW2.ravel(), db2, dw3, db3])
     return loss, grad, f["y"]
+
+
+# ------------------------------------------------------------ warm-start inputs and start
+
+def _f32(x):
+    return np.float32(x)
+
+
+def warm_start_features(step, x, p_prev, bx, psi, w_table, consts, dt):
+    """The network's 10 inputs per fluid particle, restated in float32 numpy
+    from an oracle step's exported terms (oracle.step(..., export=True)) and
+    the step's input positions x.
+
+    The inputs are built from the reference's own per-particle quantities:
+    rho_adv (predict_rho_adv, IISPH.py:281-329), a_ii (compute_term_a,
+    IISPH.py:385-428), d_ii (compute_term_d, IISPH.py:332-382), the
+    neighbour counts (IISPH.py:52-163) and the boundary share of the density
+    (compute_density, IISPH.py:177-214).  grad rho = m sum_j gradW_ij +
+    sum_b psi_b gradW_ib is recovered from d_ii = -grad rho dt^2 / rho^2.
+    ``consts``: dict with rho0, gravity, h, omega, inv_small, fluid_mass and
+    w_size (the W table's samples)."""
+    rho = np.asarray(step["rho"], np.float32)
+    rho_adv = np.asarray(step["rho_adv"], np.float32)
+    aii = np.asarray(step["a_ii"], np.float32)
+    dii = np.asarray(step["d_ii"], np.float32)
+    n = len(rho)
+    rho0, grav, h = _f32(consts["rho0"]), _f32(consts["gravity"]), _f32(consts["h"])
+    omega, inv_small, m = _f32(consts["omega"]), _f32(consts["inv_small"]), _f32(consts["fluid_mass"])
+    dt = _f32(dt)
+    dt2 = dt * dt
+    rr = rho * rho
+    inv_rho0 = _f32(1.0) / rho0
+    p_ref = _f32(1.0) / (rho0 * grav * h)
+    h2 = h * h
+    h4 = h2 * h2
+    aa = aii.copy()
+    small = (aa > -inv_small) & (aa < inv_small)
+    aa[small] = np.where(aa[small] < 0, _f32(-1.0), _f32(1.0)) * inv_small
+    p1 = np.maximum((rho0 - rho_adv) * omega / aa, _f32(0.0))
+    grad = (-dii) * (rr / dt2)[:, None]
+    # boundary share of the density: sum_b psi_b W(|x_i - x_b|) over each fluid-boundary list
+    off = np.asarray(step["fb_off"], np.int64)
+    idx = np.asarray(step["fb_idx"], np.int64)
+    xi = np.repeat(np.asarray(x, np.float32).reshape(-1, 3), np.diff(off), axis=0)
+    d = xi - np.asarray(bx, np.float32)[idx]
+    r = np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]).astype(np.float32)
+    S = int(consts["w_size"])
+    T = np.asarray(w_table, np.float32)
+    f = r * (_f32(S - 1) * (_f32(1.0) / h))
+    lo = np.minimum(f.astype(np.int64), S - 2)
+    a = f - lo.astype(np.float32)
+    w = (_f32(1.0) - a) * T[lo] + a * T[lo + 1]
+    w[r >= h] = 0
+    sWb = np.zeros(n, np.float64)
+    np.add.at(sWb, np.repeat(np.arange(n), np.diff(off)), (w * np.asarray(psi, np.float32)[idx]).astype(np.float64))
+    F = np.zeros((n, NF), np.float32)
+    F[:, 0] = rho_adv * inv_rho0 - _f32(1.0)
+    F[:, 1] = (rho_adv - rho) * inv_rho0
+    F[:, 2] = aii * rr / (dt2 * m * m) * h4 * h4
+    F[:, 3] = np.arcsinh(np.asarray(p_prev, np.float32) * p_ref)
+    F[:, 4] = np.diff(np.asarray(step["ff_off"], np.int64)).astype(np.float32)
+    F[:, 5] = sWb.astype(np.float32) * inv_rho0
+    F[:, 6] = np.sqrt((grad * grad).sum(1)).astype(np.float32) * h * inv_rho0
+    F[:, 7] = np.arcsinh(p1 * p_ref)
+    F[:, 8] = grad[:, 1] * h * inv_rho0
+    F[:, 9] = np.diff(off).astype(np.float32)
+    return F
+
+
+def solve_start(blob, feat, consts, max_rise=0.5):
+    """The pressure a learned-start step's Jacobi solve begins from
+    (replacing init_pressure, IISPH.py:166-174): the network's correction y
+    on top of u = asinh(p_prev / (rho0 g h)) (input 3, carried in float32),
+    its rise bounded by max_rise, clamped at 0 and mapped back:
+    p = sinh(max(u + min(y t_scale, max_rise), 0)) rho0 g h."""
+    feat = np.asarray(feat, np.float32)
+    y = forward(blob, feat)["y"].astype(np.float32)
+    ts = np.float32(unpack(blob)["t_scale"])
+    u = feat[:, 3]
+    p_unit = np.float32(float(consts["rho0"]) * float(consts["gravity"]) * float(consts["h"]))
+    t = np.maximum(u + np.minimum(y * ts, np.float32(max_rise)), np.float32(0.0))
+    return (np.sinh(t.astype(np.float32)) * p_unit).astype(np.float32)

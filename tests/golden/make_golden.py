@@ -1,7 +1,7 @@
 """Generate golden IISPH step vectors by running the reference's own solver.
 
 Test infrastructure only.  The reference (Mo-ZheHan/WarpSPH, read from a local
-checkout; default ``/root/reference``) is pure Python on NVIDIA Warp, which is
+checkout given by ``--reference``) is pure Python on NVIDIA Warp, which is
 not installed here.  This script imports the reference's own modules
 (``wp_sph/main.py``, ``wp_sph/solver/sph_funcs.py``, ``wp_sph/solver/IISPH.py``)
 with ``warp`` replaced by the numpy emulation in ``warp_emu.py``, patches the
@@ -10,7 +10,7 @@ module-level scene constants the reference reads at import time
 jittered state, and records per-step inputs and outputs of ``IISPH.step()``
 (``IISPH.py:1002-1371``) into ``tests/golden/<scene>.npz``.
 
-Usage:  python tests/golden/make_golden.py [--reference PATH] [scene ...]
+Usage:  python tests/golden/make_golden.py --reference PATH [scene ...]
 """
 
 from __future__ import annotations
@@ -189,7 +189,7 @@ def run_scene(ref: Path, name: str, cfg: dict) -> dict:
 
 def main_cli():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="path of a WarpSPH checkout")
     ap.add_argument("scenes", nargs="*", default=list(SCENES))
     args = ap.parse_args()
     ref = Path(args.reference)

@@ -1,0 +1,155 @@
+"""The learned warm start's inputs and the pressure each step's solve starts
+from, pinned to CPU restatements.
+
+The solve's first iterate replaces the reference's init_pressure
+(IISPH.py:166-174).  Checked here, per element, through the C ABI
+(sph_get_features, sph_get_solve_start):
+
+  * the 10 network inputs the neighbour build computes, against
+    oracle.mlp_oracle.warm_start_features restated from the FP32 oracle's
+    terms of the same step (rho_adv, a_ii, d_ii, the neighbour lists): within
+    1e-4 of max(|input|, its standard deviation in the shipped network), the
+    neighbour counts exactly;
+  * the prediction written as the first iterate, against the BF16 network
+    oracle followed by the residual/rise/clamp rule (mlp_oracle.solve_start);
+  * the continuation rule: after a capped solve the next step starts from that
+    solve's final pressure, bit for bit;
+  * the reference's p = 0 start (the first update_p from 0) and the 0.5 p_prev
+    start.
+"""
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as M
+from tests.helpers import elemstats, parity_floors
+
+pytestmark = pytest.mark.gpu
+
+FEATURE_TOL = 1e-4
+
+
+def _consts(params):
+    return dict(rho0=params.rho0, gravity=params.gravity, h=params.h, omega=params.omega,
+                inv_small=params.inv_small, fluid_mass=params.fluid_mass, w_size=params.w_table_size)
+
+
+def _recording_solver(params, scene):
+    from warpsph_b200 import _lib
+    from warpsph_b200.solver import IISPH
+
+    sol = IISPH(stage_path=None, params=params.replace(keep_fb_lists=True), scene=scene)
+    _lib.check(sol._ctx, sol._lib.sph_set_record_features(sol._ctx, 1))
+    return sol
+
+
+def _features_and_start(sol):
+    from warpsph_b200 import _lib
+
+    f = np.zeros((sol.n, _lib.SPH_MLP_FEATURES), np.float32)
+    p0 = np.zeros(sol.n, np.float32)
+    _lib.check(sol._ctx, sol._lib.sph_get_features(sol._ctx, _lib.ptr(f), None))
+    _lib.check(sol._ctx, sol._lib.sph_get_solve_start(sol._ctx, _lib.ptr(p0)))
+    return f, p0
+
+
+def _oracle_step(oracle, params, x, v, bx, psi, dt):
+    from warpsph_b200.tables import kernel_tables
+
+    op = oracle.reference_params(diameter=params.diameter, gravity=params.gravity, w_size=params.w_table_size,
+                                 g_size=params.g_table_size)
+    return oracle.step(op, x, v, bx, None, psi, dt, 1.0 / dt, tables=kernel_tables(params))
+
+
+def test_learned_inputs_and_prediction_vs_oracle(oracle):
+    """8,000-particle dam break, learned start with continuation (the
+    benchmark's headline mode), 40 steps in: one step's inputs and first
+    iterate against the restatements."""
+    from warpsph_b200 import _lib
+    from warpsph_b200.learned import load_blob
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+    from warpsph_b200.tables import kernel_tables
+
+    params = preset_params("dam_break_8k", warm_start="mlp", warm_continue=True)
+    scene = preset_scene("dam_break_8k")
+    sol = _recording_solver(params, scene)
+    sol.steps(40)
+    x, v, p_prev, dt = sol.x.numpy(), sol.v.numpy(), sol.p.numpy(), sol.dt
+    psi = sol.boundary_phi.numpy()
+    capped_before = bool(sol.last_stats["flags"] & _lib.SPH_F_NOT_CONVERGED)
+    sol.step()
+    f_gpu, p0_gpu = _features_and_start(sol)
+    sol.close()
+
+    ref = _oracle_step(oracle, params, x, v, scene.boundary_x, psi, dt)
+    f_ref = M.warm_start_features(ref, x, p_prev, scene.boundary_x, psi, kernel_tables(params)[0],
+                                  _consts(params), dt)
+    blob = load_blob()
+    sd = blob[10:20]
+    assert np.array_equal(f_gpu[:, 4], f_ref[:, 4]) and np.array_equal(f_gpu[:, 9], f_ref[:, 9])
+    worst = {}
+    for k in range(10):
+        err = np.abs(f_gpu[:, k].astype(np.float64) - f_ref[:, k]) / np.maximum(np.abs(f_ref[:, k]), sd[k])
+        worst[k] = float(err.max())
+    assert max(worst.values()) < FEATURE_TOL, worst
+
+    # the first iterate: the network on the library's own inputs, then the
+    # rule (or, after a capped solve, that solve's pressure)
+    if capped_before:
+        assert np.array_equal(p0_gpu, p_prev)
+    else:
+        want = M.solve_start(blob, f_gpu, _consts(params))
+        mx, p999 = elemstats(p0_gpu, want, parity_floors(params, dt)["p"])
+        assert p999 < 1e-4 and mx < 1e-3, (mx, p999)
+
+
+def test_continuation_starts_from_capped_pressure():
+    """warm_continue: a solve stopped at the iteration cap hands its final
+    pressure to the next step unchanged (in the new sorted order)."""
+    from warpsph_b200 import _lib
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+
+    params = preset_params("dam_break_8k", warm_start="mlp", warm_continue=True, max_loop=3)
+    sol = _recording_solver(params, preset_scene("dam_break_8k"))
+    sol.step()
+    assert sol.last_stats["flags"] & _lib.SPH_F_NOT_CONVERGED
+    p_final = sol.p.numpy()
+    sol.step()
+    _, p0 = _features_and_start(sol)
+    assert np.array_equal(p0, p_final)
+    sol.close()
+
+
+def test_reference_and_half_starts(oracle):
+    """p = 0 (the reference, IISPH.py:173): the solve starts at the first
+    update_p from 0, max((rho0 - rho_adv) omega / a_ii, 0); 0.5 p_prev
+    (IISPH.py:174): half the carried pressure, exactly."""
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+
+    scene = preset_scene("dam_break_8k")
+    params = preset_params("dam_break_8k")
+    sol = _recording_solver(params, scene)
+    sol.steps(20)
+    x, v, dt = sol.x.numpy(), sol.v.numpy(), sol.dt
+    psi = sol.boundary_phi.numpy()
+    sol.step()
+    _, p0 = _features_and_start(sol)
+    sol.close()
+    ref = _oracle_step(oracle, params, x, v, scene.boundary_x, psi, dt)
+    rho0, omega, small = np.float32(params.rho0), np.float32(params.omega), np.float32(params.inv_small)
+    aa = ref["a_ii"].copy()
+    tiny = (aa > -small) & (aa < small)
+    aa[tiny] = np.where(aa[tiny] < 0, np.float32(-1), np.float32(1)) * small
+    want = np.maximum((rho0 - ref["rho_adv"]) * omega / aa, np.float32(0))
+    mx, p999 = elemstats(p0, want, parity_floors(params, dt)["p"])
+    assert mx < 1e-4, (mx, p999)
+
+    half = _recording_solver(params.replace(warm_start="half"), scene)
+    half.steps(20)
+    p_prev = half.p.numpy()
+    half.step()
+    _, p0 = _features_and_start(half)
+    assert np.array_equal(p0, p_prev / np.float32(2))
+    half.close()

@@ -106,6 +106,7 @@ SIGNATURES = {
     "sph_build_tables": (ctypes.c_int, [ctypes.POINTER(SphParams), _P, _P]),
     "sph_set_boundary": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64]),
     "sph_set_fluid": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64]),
+    "sph_update_fluid": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int64]),
     "sph_set_pressure": (ctypes.c_int, [_P, _P, ctypes.c_int64]),
     "sph_step": (ctypes.c_int, [_P, ctypes.POINTER(SphStepStats)]),
     "sph_steps": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(SphStepStats)]),
@@ -130,9 +131,13 @@ SIGNATURES = {
     "sph_set_mlp": (ctypes.c_int, [_P, _P, ctypes.c_int32]),
     "sph_set_record_features": (ctypes.c_int, [_P, ctypes.c_int32]),
     "sph_get_features": (ctypes.c_int, [_P, _P, _P]),
+    "sph_get_solve_start": (ctypes.c_int, [_P, _P]),
     "sph_mlp_train": (ctypes.c_int, [ctypes.POINTER(SphMlpTrainConfig), _P, _P, ctypes.c_int64, _P, _P]),
     "sph_mlp_eval": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, ctypes.c_int32, _P, _P]),
     "sph_boundary_psi_noalloc": (ctypes.c_int, [ctypes.POINTER(SphParams), _P, ctypes.c_int64, _P, _P, _P]),
+    "sph_sample_solid": (ctypes.c_int, [_P, ctypes.c_int64, _P, ctypes.c_int64, _P, ctypes.c_int32, _P,
+                                        ctypes.c_int32, _P, ctypes.c_int32, _P, _P, _P, ctypes.c_int64, _P,
+                                        ctypes.c_int32]),
     "sph_num_fluid": (ctypes.c_int64, [_P]),
     "sph_num_boundary": (ctypes.c_int64, [_P]),
     "sph_stream": (ctypes.c_void_p, [_P]),

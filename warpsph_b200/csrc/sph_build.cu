@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(256) k_psi(PsiArgs a, float* psi) {
   const Grid& g = fr.g;
   const float4 xb = a.bpos[b];
   const int3 ci = cell_coord(g, xb.x, xb.y, xb.z);
-  float rho = c.w0;
+  float rho = a.w0_from_table ? __ldg(a.w_table) : c.w0;
   const int x0 = max(ci.x - kXReach, 0), x1 = min(ci.x + kXReach, g.nx - 1);
   for (int cz = max(ci.z - 1, 0); cz <= min(ci.z + 1, g.nz - 1); ++cz)
     for (int cy = max(ci.y - 1, 0); cy <= min(ci.y + 1, g.ny - 1); ++cy) {

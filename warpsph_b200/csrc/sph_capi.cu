@@ -71,6 +71,7 @@ struct SphCtx {
   float *p_a = nullptr, *p_b = nullptr, *Ap = nullptr;
   float* pmlp = nullptr;
   float* feat = nullptr;             // learned warm-start inputs, kFeatures per particle
+  float* p_start = nullptr;          // the solve's starting iterate, kept while recording features
   sph::MlpPacked* mlp = nullptr;     // packed network weights
   bool have_mlp = false;
   bool record_feat = false;
@@ -479,6 +480,7 @@ int alloc_fluid(SphCtx* ctx, int64_t n) {
   CK(dalloc(ctx->pmlp, m));
   CK(dalloc(ctx->stage, 7 * m));
   CK(dalloc(ctx->feat, size_t(sph::kFeatures) * m));
+  CK(dalloc(ctx->p_start, m));
   CK(cudaMemset(ctx->rho, 0, sizeof(float) * m));
   CK(cudaMemset(ctx->bvec, 0, sizeof(float4) * m));
   CK(cudaMemset(ctx->dii_aii, 0, sizeof(float4) * m));
@@ -586,6 +588,11 @@ int enqueue_warm(SphCtx* ctx) {
     }
     CK(sph::launch_mlp_infer_tc(m, ctx->sm_count, ctx->stream));
   }
+  // while features are recorded, keep the iterate the solve starts from
+  // (sph_get_solve_start): p_1 from the build or the network, or 0.5 p_prev
+  if (ctx->record_feat && ctx->n > 0)
+    CK(cudaMemcpyAsync(ctx->p_start, ctx->p_a, sizeof(float) * size_t(ctx->n), cudaMemcpyDeviceToDevice,
+                       ctx->stream));
   return SPH_OK;
 }
 
@@ -849,7 +856,7 @@ void sph_destroy(SphCtx* ctx) {
                   ctx->pos_w, ctx->vel_w, ctx->orig_s, ctx->orig_w, ctx->p_s, ctx->pprev_w, ctx->key, ctx->rank,
                   ctx->sort_src, ctx->sort_orig, ctx->cell_count, ctx->cell_start, ctx->scan_part, ctx->nbr_ff,
                   ctx->cnt_ff, ctx->nbr_fb, ctx->cnt_fb, ctx->rho, ctx->bvec, ctx->dii_aii, ctx->vadv, ctx->a4,
-                  ctx->p_a, ctx->p_b, ctx->Ap, ctx->pmlp, ctx->feat, ctx->mlp, ctx->stage, ctx->partials, ctx->st, ctx->acc, ctx->ring,
+                  ctx->p_a, ctx->p_b, ctx->Ap, ctx->pmlp, ctx->feat, ctx->p_start, ctx->mlp, ctx->stage, ctx->partials, ctx->st, ctx->acc, ctx->ring,
                   ctx->d_scenes, ctx->d_chunks, ctx->d_chunk_scene,
                   ctx->last};
   for (void* p : ptrs)
@@ -960,6 +967,23 @@ int sph_set_fluid(SphCtx* ctx, const float* x3, const float* v3, int64_t n) {
                               ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
   }
+  return SPH_OK;
+}
+
+int sph_update_fluid(SphCtx* ctx, const float* x3, const float* v3, const float* p, int64_t n) {
+  if (!ctx || n != ctx->n || (n > 0 && (!x3 || !v3 || !p)))
+    return fail(ctx, SPH_E_INVALID, "sph_update_fluid replaces x, v and p of the current particles (n = fluid count)");
+  CK(cudaSetDevice(ctx->dev));
+  if (n == 0) return SPH_OK;
+  // the grid, dt, simulated time and the per-scene cap flags stay as they are
+  float* sx = ctx->stage;
+  float* sv = ctx->stage + 3 * n;
+  float* sp = ctx->stage + 6 * n;
+  CK(cudaMemcpyAsync(sx, x3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(sv, v3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(sp, p, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
+  CK(sph::launch_pack_fluid(int(n), 0, sx, sv, ctx->pos_s, ctx->vel_s, ctx->orig_s, ctx->p_s, ctx->stream, sp));
+  CK(cudaStreamSynchronize(ctx->stream));
   return SPH_OK;
 }
 
@@ -1439,6 +1463,22 @@ int sph_get_features(SphCtx* ctx, float* feat, float* target) {
     const double unit = 1.0 / (ctx->P.rho0 * ctx->P.gravity * ctx->P.h);
     for (int64_t k = 0; k < n; ++k) target[ow[k]] = float(std::asinh(double(h[k]) * unit));
   }
+  return SPH_OK;
+}
+
+int sph_get_solve_start(SphCtx* ctx, float* p) {
+  if (!ctx || !p) return SPH_E_INVALID;
+  if (!ctx->record_feat)
+    return fail(ctx, SPH_E_INVALID, "the solve's start is only kept with sph_set_record_features(ctx, 1)");
+  CK(cudaSetDevice(ctx->dev));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const int64_t n = ctx->n;
+  if (n == 0) return SPH_OK;
+  std::vector<int> ow(n);
+  std::vector<float> h(n);
+  CK(cudaMemcpy(ow.data(), ctx->orig_w, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(h.data(), ctx->p_start, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  for (int64_t k = 0; k < n; ++k) p[ow[k]] = h[k];
   return SPH_OK;
 }
 

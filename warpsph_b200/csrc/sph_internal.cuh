@@ -442,6 +442,7 @@ struct PsiArgs {
   const float* w_table;
   float4* bpos;            // in: x,y,z; out: w = psi
   const int* bcell_start;
+  int w0_from_table;       // 1: W(0) is read from w_table[0] on the device instead of c.w0
 };
 
 // launchers (host)
@@ -461,7 +462,7 @@ cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, bool spline, i
 cudaError_t launch_jacobi(const JacobiArgs& a, int grid, int block, int ppt, int unroll, size_t smem,
                           cudaStream_t s);
 cudaError_t launch_pack_fluid(int n, int base, const float* x3, const float* v3, float4* pos, float4* vel,
-                              int* orig, float* p, cudaStream_t s);
+                              int* orig, float* p, cudaStream_t s, const float* p_in = nullptr);
 cudaError_t launch_unsort4(int n, const int* orig, const float4* src, int component, float* out, cudaStream_t s);
 cudaError_t launch_unsort1(int n, const int* orig, const float* src, float* out, cudaStream_t s);
 cudaError_t launch_sort1(int n, const int* orig, const float* src, float* out, cudaStream_t s);

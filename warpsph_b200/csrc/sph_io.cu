@@ -7,17 +7,18 @@
 namespace sph {
 
 // Particles [base, base + n) of the state from packed host-order float3
-// arrays; their original ids are base + (index in the arrays).
+// arrays (and pressures, NULL = 0); their original ids are base + (index in
+// the arrays).
 __global__ void k_pack_fluid(int n, int base, const float* __restrict__ x3, const float* __restrict__ v3,
-                             float4* __restrict__ pos, float4* __restrict__ vel, int* __restrict__ orig,
-                             float* __restrict__ p) {
+                             const float* __restrict__ p_in, float4* __restrict__ pos, float4* __restrict__ vel,
+                             int* __restrict__ orig, float* __restrict__ p) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int k = base + i;
   pos[k] = make_float4(x3[3 * i], x3[3 * i + 1], x3[3 * i + 2], 0.f);
   vel[k] = v3 ? make_float4(v3[3 * i], v3[3 * i + 1], v3[3 * i + 2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
   orig[k] = k;
-  p[k] = 0.f;
+  p[k] = p_in ? p_in[i] : 0.f;
 }
 
 // out[orig[k]] = src[k].xyz  (component = -1)  or  src[k].{x,y,z,w}[component]
@@ -49,9 +50,9 @@ __global__ void k_sort1(int n, const int* __restrict__ orig, const float* __rest
 }
 
 cudaError_t launch_pack_fluid(int n, int base, const float* x3, const float* v3, float4* pos, float4* vel,
-                              int* orig, float* p, cudaStream_t s) {
+                              int* orig, float* p, cudaStream_t s, const float* p_in) {
   if (n <= 0) return cudaSuccess;
-  k_pack_fluid<<<(n + 255) / 256, 256, 0, s>>>(n, base, x3, v3, pos, vel, orig, p);
+  k_pack_fluid<<<(n + 255) / 256, 256, 0, s>>>(n, base, x3, v3, p_in, pos, vel, orig, p);
   return cudaGetLastError();
 }
 

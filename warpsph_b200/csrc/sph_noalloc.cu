@@ -2,12 +2,11 @@
 //
 // Who needs this: callers that are not allowed to call cudaMalloc.  Typical
 // cases are a host framework that owns all device memory through its own
-// pool and forbids foreign allocations, code running while another component
-// is capturing a CUDA graph in a mode that rejects allocation calls, and
-// embedded/real-time callers that must not allocate after start-up because an
-// allocation can block or fail at an arbitrary time.  Such a caller allocates
-// its inputs and outputs itself and needs the library to bring its own
-// scratch memory.
+// pool and forbids foreign allocations (an allocation behind its back can fail
+// or fragment memory it has already handed out), and embedded or real-time
+// callers that must not allocate after start-up because an allocation can
+// block or fail at an arbitrary time.  Such a caller allocates its inputs and
+// outputs itself and needs the library to bring its own scratch memory.
 //
 // sph_boundary_psi_noalloc computes the same psi as sph_set_boundary (the
 // reference's compute_boundary_density, IISPH.py:23-49), but its scratch — the
@@ -19,6 +18,10 @@
 // per-cell counters are cleared at the start of every call, everything else is
 // fully overwritten.  Two calls whose work overlaps on the GPU (different
 // streams, or different host threads without ordering) race on the array.
+// The array's device address is looked up once per device, on that device's
+// first call, and kept: after a cudaDeviceReset of that device the module is
+// loaded anew and the kept address is stale, so the entry point must not be
+// used on a device after it has been reset.
 #include <algorithm>
 #include <cmath>
 #include <mutex>
@@ -31,6 +34,8 @@ namespace {
 constexpr long long kMaxB = SPH_NOALLOC_MAX_BOUNDARY;
 constexpr long long kMaxCells = SPH_NOALLOC_MAX_CELLS;
 constexpr long long kScanParts = kMaxCells / 4096 + 2;
+// largest explicit domain extent accepted, in support radii per axis
+constexpr double kMaxDomainCells = 1e7;
 
 // byte offsets inside the scratch array (each 256-byte aligned)
 constexpr long long al(long long b) { return (b + 255) / 256 * 256; }
@@ -131,7 +136,20 @@ extern "C" int sph_boundary_psi_noalloc(const SphParams* params, const float* d_
   using namespace sph;
   if (!params || nb < 0 || (nb > 0 && (!d_xb3 || !d_w_table || !d_psi))) return SPH_E_INVALID;
   if (nb > kMaxB) return SPH_E_TOO_LARGE;  // more than SPH_NOALLOC_MAX_BOUNDARY particles
-  if (!(params->h > 0) || params->w_table_size < 2) return SPH_E_INVALID;
+  if (!(params->h > 0) || !std::isfinite(params->h) || params->w_table_size < 2) return SPH_E_INVALID;
+  if (!std::isfinite(params->rho0)) return SPH_E_INVALID;
+  // an explicit grid extent must be finite and not absurdly many cells wide:
+  // the cell count below is computed from it before any kernel is launched
+  bool have_domain = false;
+  for (int a = 0; a < 3; ++a) {
+    const double dmin = params->domain_min[a], dmax = params->domain_max[a];
+    if (!std::isfinite(dmin) || !std::isfinite(dmax)) return SPH_E_INVALID;
+    have_domain = have_domain || (dmax > dmin);
+  }
+  if (have_domain)
+    for (int a = 0; a < 3; ++a)
+      if (params->domain_max[a] - params->domain_min[a] > kMaxDomainCells * params->h)
+        return SPH_E_INVALID;
   if (nb == 0) return SPH_OK;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SPH_E_CUDA;
@@ -150,9 +168,8 @@ extern "C" int sph_boundary_psi_noalloc(const SphParams* params, const float* d_
   if (cudaGetLastError() != cudaSuccess) return SPH_E_CUDA;
 
   // grid extent: params.domain when given, else the points' bounding box
+  // (read back to the host: this synchronises `stream`)
   double lo[3], hi[3];
-  bool have_domain = false;
-  for (int a = 0; a < 3; ++a) have_domain = have_domain || (params->domain_max[a] > params->domain_min[a]);
   if (have_domain) {
     for (int a = 0; a < 3; ++a) {
       lo[a] = params->domain_min[a];
@@ -168,17 +185,27 @@ extern "C" int sph_boundary_psi_noalloc(const SphParams* params, const float* d_
       hi[a] = hb[a] <= hb[3 + a] ? hb[3 + a] : 0.0;
     }
   }
+  // Cell counts are formed in double (the extents are finite: checked above,
+  // or the bounding box of finite coordinates), so nothing overflows before
+  // the comparison; each pass grows the cell by 1.25, so the loop ends.
   double cell = double(float(params->h)) * 1.01;
   const double pad = 2.0 * params->h;
   long long dims[3], tot;
   for (;;) {
-    tot = 1;
+    double dd[3], td = 1.0;
     for (int a = 0; a < 3; ++a) {
       const double w = a == 0 ? cell / kXSplit : cell;
-      dims[a] = std::max<long long>(1, (long long)std::ceil((hi[a] - lo[a] + 2 * pad) / w) + 1);
-      tot *= dims[a];
+      dd[a] = std::max(1.0, std::ceil((hi[a] - lo[a] + 2 * pad) / w) + 1.0);
+      td *= dd[a];
     }
-    if (tot <= kMaxCells) break;
+    if (td <= double(kMaxCells)) {
+      tot = 1;
+      for (int a = 0; a < 3; ++a) {
+        dims[a] = (long long)dd[a];
+        tot *= dims[a];
+      }
+      break;
+    }
     cell *= 1.25;  // coarser cells keep the search complete
   }
   Grid g{};
@@ -218,14 +245,11 @@ extern "C" int sph_boundary_psi_noalloc(const SphParams* params, const float* d_
   pa.c.sw = params->w_table_size;
   pa.c.w_scale = float(params->w_table_size - 1) * float(1.0 / params->h);
   pa.c.rho0 = float(params->rho0);
-  // spline_W(0) = W_table[0]: fetched from the caller's table on the device
   pa.w_table = d_w_table;
+  // spline_W(0) = W_table[0], read by the kernel from the caller's table
+  pa.w0_from_table = 1;
   pa.bpos = pos_sorted;
   pa.bcell_start = sa.cell_start;
-  float w0 = 0.f;
-  if (cudaMemcpyAsync(&w0, d_w_table, sizeof(float), cudaMemcpyDeviceToHost, s) != cudaSuccess) return SPH_E_CUDA;
-  if (cudaStreamSynchronize(s) != cudaSuccess) return SPH_E_CUDA;
-  pa.c.w0 = w0;
   if (launch_psi_sorted(pa, psi_sorted, 256, s) != cudaSuccess) return SPH_E_CUDA;
   if (launch_unsort1(n, sorted_orig, psi_sorted, d_psi, s) != cudaSuccess) return SPH_E_CUDA;
   return SPH_OK;

@@ -19,6 +19,7 @@ import warnings
 import numpy as np
 
 from . import _lib
+from .frames import FrameRecorder
 from .params import SolverParams
 from .scenes import Scene, box_scene
 from .tables import kernel_tables
@@ -47,26 +48,6 @@ class DeviceField:
 
     def __repr__(self):
         return f"DeviceField({self._name}, shape={self.shape})"
-
-
-class FrameRecorder:
-    """Headless stand-in for the reference's UsdRenderer (IISPH.py:824-827): keeps
-    fluid positions per rendered frame and writes them to ``<stage_path>.npz``."""
-
-    def __init__(self, stage_path: str, fps: int):
-        self.stage_path = stage_path
-        self.fps = fps
-        self.times: list[float] = []
-        self.frames: list[np.ndarray] = []
-
-    def add(self, t: float, x: np.ndarray):
-        self.times.append(t)
-        self.frames.append(x)
-
-    def save(self):
-        path = self.stage_path if self.stage_path.endswith(".npz") else self.stage_path + ".npz"
-        np.savez_compressed(path, times=np.asarray(self.times), x=np.stack(self.frames) if self.frames else np.zeros(0))
-        return path
 
 
 def _reference_constants():
@@ -100,15 +81,37 @@ class IISPH:
         self._ctx = None
         self._lib = _lib.load()
 
+        rigid_v = None
         if scene is None:
+            # IISPH.py:749-766: the fluid block of each scene type
+            stype = getattr(main, "scene_type", None)
+            name = getattr(stype, "name", "EMPTY")
             bw, bh, bl = box
-            min_point = (bw * 0.02, bh * 0.02, bl * 0.02)
-            max_point = (bw * 0.98, bh * 0.4, bl * 0.55)
-            self.init_particles(min_point, max_point)
+            layers = 3
+            if name == "HOUSE":
+                min_point, max_point = (bw * 0.7, bh * 0.01, bl * 0.8), (bw * 0.99, bh * 0.5, bl * 0.99)
+            elif name == "PLANE":
+                min_point, max_point = (bw * 0.45, bh * 0.05, bl * 0.05), (bw * 0.55, bh * 0.95, bl * 0.95)
+                layers = 0
+            elif name == "HAND":
+                min_point, max_point = (bw * 0.48, bh * 0.05, bl * 0.48), (bw * 0.52, bh * 0.99, bl * 0.52)
+            else:
+                min_point, max_point = (bw * 0.02, bh * 0.02, bl * 0.02), (bw * 0.98, bh * 0.4, bl * 0.55)
+            self.init_particles(min_point, max_point, boundary_layers=layers)
+            models = getattr(main, "SCENE_MODELS", {}).get(stype, []) if main is not None else []
+            if models:
+                self._add_models(models)
+            rigid_v = getattr(main, "RIGID_VELOCITY", {}).get(stype) if main is not None else None
+            if rigid_v is not None:
+                # the rigid body moves (DYNAMIC_SCENE, main.py:20; update_rigid_x, IISPH.py:1356-1365)
+                self.params = params = params.replace(move_boundary=True)
         else:
             self._set_scene(scene)
 
         self._create_context()
+        if rigid_v is not None:
+            # set_rigid_v at sim_time 0 (IISPH.py:1061-1081), before the first step
+            self.set_rigid_velocity(rigid_v)
 
         self.renderer = FrameRecorder(stage_path, self._fps) if stage_path else None
         if preview:
@@ -139,6 +142,20 @@ class IISPH:
             self._upload()
         print(f"Initialized {self.n} fluid and {self.boundary_n} boundary particles")
 
+    def _add_models(self, models):
+        """Mesh models sampled into rigid boundary particles after the box
+        walls (IISPH.py:945-991, model.py:53-60)."""
+        from .model import load_model
+
+        pts = [load_model(f, scale, np.asarray(pos, np.float64), np.asarray(rot, np.float64),
+                          spacing=self.params.diameter, device=self.params.device)
+               for f, scale, pos, rot in models]
+        for f, p in zip(models, pts):
+            print(f"Loaded model {f[0]} with {len(p)} particles")
+        s = self._scene
+        bx = np.concatenate([s.boundary_x] + [np.asarray(p, np.float32) for p in pts]).astype(np.float32)
+        self._set_scene(Scene(s.fluid_x, s.fluid_v, bx, s.boundary_hide_n, s.box))
+
     def _set_scene(self, scene: Scene):
         self._scene = scene
         self.n = scene.n
@@ -157,6 +174,15 @@ class IISPH:
         self._scene = Scene(x, v, self._scene.boundary_x, self._scene.boundary_hide_n, self._scene.box)
         self.n = len(x)
         _lib.check(self._ctx, self._lib.sph_set_fluid(self._ctx, _lib.ptr(x), _lib.ptr(v), self.n))
+
+    def update_state(self, x, v, p):
+        """Replace positions, velocities and pressures (original order) of the
+        current particles, keeping dt, time and the solver's history
+        (sph_update_fluid); set_state instead starts a new state."""
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 3)
+        v = np.ascontiguousarray(v, dtype=np.float32).reshape(-1, 3)
+        p = np.ascontiguousarray(p, dtype=np.float32).reshape(-1)
+        _lib.check(self._ctx, self._lib.sph_update_fluid(self._ctx, _lib.ptr(x), _lib.ptr(v), _lib.ptr(p), len(x)))
 
     def add_fluid(self, x, v=None):
         """Append fluid particles (e.g. an emitter's new layer) to the state on
@@ -336,7 +362,8 @@ class IISPH:
         if self.renderer is None:
             return
         if self.sim_time - self.last_frame_time >= self.frame_dt:
-            self.renderer.add(self.sim_time, self.x.numpy())
+            rigid = self.boundary_x.numpy()[self.boundary_hide_n:]
+            self.renderer.add(self.sim_time, self.x.numpy(), rigid)
             self.last_frame_time = self.sim_time
 
     def raise_error(self, message):
