@@ -291,23 +291,26 @@ int sph_boundary_psi_noalloc(const SphParams* params, const float* d_xb3, int64_
  * computes and uses it as the solve's first iterate; the unchanged Jacobi
  * loop (at least 2 iterations, average density error <= eta) still decides
  * convergence.
- * The network is residual on the previous step's pressure: with input 3,
- * u = asinh(p_prev / (rho0 g h)), taken in FP32 (no BF16 rounding on the
- * skip path), the prediction is
+ * The network is residual on a base taken in FP32 (no BF16 rounding on the
+ * skip path): u = max(input 3, input 10), the larger of the previous step's
+ * pressure, asinh(p_prev / (rho0 g h)), and the hydrostatic pressure of the
+ * fluid column above the particle, asinh(depth / h) (depth = highest fluid
+ * particle of the particle's neighbour-grid column (x, z) minus its own y).
+ * The prediction is
  *   p = sinh(max(u + min(y * t_scale, SPH_MLP_MAX_RISE), 0)) * rho0 * g * h;
  * the bounded rise keeps one over-predicted particle (which the solve's test,
  * counting only compressed particles, would not see) from being kicked out.
  * Weights travel as one FP32 blob of SPH_MLP_BLOB floats:
- *   mu[10], sd[10]   input standardisation (x - mu) / sd
+ *   mu[11], sd[11]   input standardisation (x - mu) / sd
  *   t_scale          output unit of y
- *   W1[10][64] b1[64] W2[64][64] b2[64] w3[64] b3   (SPH_MLP_PARAMS, W[in][out])
+ *   W1[11][64] b1[64] W2[64][64] b2[64] w3[64] b3   (SPH_MLP_PARAMS, W[in][out])
  * sph_get_features gives t = asinh(p / (rho0 g h)) of the converged pressure
  * (pressures span orders of magnitude; asinh keeps them on one scale); the
  * network is trained on the residual t - u.  sph_mlp_train and sph_mlp_eval
  * regress y * t_scale on whatever target array they are given. */
-#define SPH_MLP_FEATURES 10
-#define SPH_MLP_PARAMS 4929
-#define SPH_MLP_BLOB 4950
+#define SPH_MLP_FEATURES 11
+#define SPH_MLP_PARAMS 4993
+#define SPH_MLP_BLOB 5016
 #define SPH_MLP_MAX_RISE 0.5f
 
 typedef struct SphMlpTrainConfig {
@@ -332,6 +335,12 @@ int sph_get_features(SphCtx* ctx, float* feat, float* target);
  * extra Ap_0 pass), and with SPH_WARM_MLP the network's prediction or, after
  * a capped solve with warm_continue, that solve's final pressure. */
 int sph_get_solve_start(SphCtx* ctx, float* p);
+/* The neighbour grid of scene `scene` (0 for a single scene), for tools that
+ * restate per-cell quantities: out[0..2] origin xyz, out[3] 1 / cell size
+ * (y, z), out[4] 1 / cell size along x (half cells), out[5..7] cells along
+ * x, y, z, out[8] the scene's first global cell id.  Float fields hold the
+ * float32 values the kernels use. */
+int sph_get_grid(SphCtx* ctx, int32_t scene, double* out9);
 /* Train in place: Adam on mean squared error over shuffled minibatches, on the
  * GPU with the library's own forward/backward kernels.  blob supplies mu, sd,
  * t_scale and the initial weights; epoch_loss (epochs floats) may be NULL. */

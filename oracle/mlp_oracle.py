@@ -7,7 +7,7 @@ back-propagated layer-2/layer-1 deltas are rounded to bfloat16 (round to
 nearest even) before each product; sums are taken in float64 here (the GPU
 accumulates in FP32, which is the difference the tests tolerate).
 
-Blob layout (include/wpsph.h): mu[10], sd[10], t_scale, then W1[10][64],
+Blob layout (include/wpsph.h): mu[11], sd[11], t_scale, then W1[11][64],
 b1[64], W2[64][64], b2[64], w3[64], b3 with W[in][out].
 """
 
@@ -15,9 +15,9 @@ from __future__ import annotations
 
 import numpy as np
 
-NF, NH = 10, 64
-OFF_MU, OFF_SD, OFF_TS = 0, 10, 20
-P0 = 21
+NF, NH = 11, 64
+OFF_MU, OFF_SD, OFF_TS = 0, NF, 2 * NF
+P0 = 2 * NF + 1
 SIZES = [("W1", (NF, NH)), ("b1", (NH,)), ("W2", (NH, NH)), ("b2", (NH,)), ("w3", (NH,)), ("b3", (1,))]
 NPARAMS = sum(int(np.prod(s)) for _, s in SIZES)
 BLOB = P0 + NPARAMS
@@ -89,8 +89,25 @@ def _f32(x):
     return np.float32(x)
 
 
-def warm_start_features(step, x, p_prev, bx, psi, w_table, consts, dt):
-    """The network's 10 inputs per fluid particle, restated in float32 numpy
+def column_top_depth(x, grid):
+    """Input 10's depth: per fluid particle, the highest fluid y of its
+    neighbour-grid column (x, z) minus its own y, clamped at 0.  ``grid`` is
+    sph_get_grid's output (origin, 1 / cell (y, z), 1 / cell along x, cells
+    per axis); cell coordinates are float32 floor((x - origin) / cell),
+    clamped to the grid, as the library computes them."""
+    x = np.asarray(x, np.float32).reshape(-1, 3)
+    ox, oy, oz, inv, inv_x = (np.float32(g) for g in grid[:5])
+    nx, ny, nz = (int(g) for g in grid[5:8])
+    cx = np.clip(np.floor((x[:, 0] - ox) * inv_x), 0, nx - 1).astype(np.int64)
+    cz = np.clip(np.floor((x[:, 2] - oz) * inv), 0, nz - 1).astype(np.int64)
+    col = cz * nx + cx
+    top = np.full(nx * nz, -np.inf, np.float32)
+    np.maximum.at(top, col, x[:, 1])
+    return np.maximum(top[col] - x[:, 1], np.float32(0))
+
+
+def warm_start_features(step, x, p_prev, bx, psi, w_table, consts, dt, grid):
+    """The network's 11 inputs per fluid particle, restated in float32 numpy
     from an oracle step's exported terms (oracle.step(..., export=True)) and
     the step's input positions x.
 
@@ -101,7 +118,8 @@ def warm_start_features(step, x, p_prev, bx, psi, w_table, consts, dt):
     (compute_density, IISPH.py:177-214).  grad rho = m sum_j gradW_ij +
     sum_b psi_b gradW_ib is recovered from d_ii = -grad rho dt^2 / rho^2.
     ``consts``: dict with rho0, gravity, h, omega, inv_small, fluid_mass and
-    w_size (the W table's samples)."""
+    w_size (the W table's samples); ``grid``: sph_get_grid's output (input 10,
+    column_top_depth)."""
     rho = np.asarray(step["rho"], np.float32)
     rho_adv = np.asarray(step["rho_adv"], np.float32)
     aii = np.asarray(step["a_ii"], np.float32)
@@ -147,19 +165,21 @@ def warm_start_features(step, x, p_prev, bx, psi, w_table, consts, dt):
     F[:, 7] = np.arcsinh(p1 * p_ref)
     F[:, 8] = grad[:, 1] * h * inv_rho0
     F[:, 9] = np.diff(off).astype(np.float32)
+    F[:, 10] = np.arcsinh(column_top_depth(x, grid) / h)
     return F
 
 
 def solve_start(blob, feat, consts, max_rise=0.5):
     """The pressure a learned-start step's Jacobi solve begins from
     (replacing init_pressure, IISPH.py:166-174): the network's correction y
-    on top of u = asinh(p_prev / (rho0 g h)) (input 3, carried in float32),
-    its rise bounded by max_rise, clamped at 0 and mapped back:
+    on top of the base u = max(input 3, input 10) (the previous step's
+    pressure and the column's hydrostatic pressure, carried in float32), its
+    rise bounded by max_rise, clamped at 0 and mapped back:
     p = sinh(max(u + min(y t_scale, max_rise), 0)) rho0 g h."""
     feat = np.asarray(feat, np.float32)
     y = forward(blob, feat)["y"].astype(np.float32)
     ts = np.float32(unpack(blob)["t_scale"])
-    u = feat[:, 3]
+    u = np.maximum(feat[:, 3], feat[:, 10])
     p_unit = np.float32(float(consts["rho0"]) * float(consts["gravity"]) * float(consts["h"]))
     t = np.maximum(u + np.minimum(y * ts, np.float32(max_rise)), np.float32(0.0))
     return (np.sinh(t.astype(np.float32)) * p_unit).astype(np.float32)

@@ -101,3 +101,21 @@ def elemstats(a, b, floor, x_like=False):
     if e.size == 0:
         return 0.0, 0.0
     return float(e.max()), float(np.percentile(e, 99.9))
+
+
+# The relaxed-Jacobi outputs (p, s, Ap) of an FP32 evaluation move by ~5e-4 of
+# a single particle's value with the summation order alone (the update divides
+# the small residual rho0 - rho_adv - Ap by a_ii); a result counts as matching
+# when it is within 1e-4 of the reference or no further from the FP64 oracle
+# than NOISE times the reference's own FP32 result is.
+NOISE = 4.0
+
+
+def jacobi_output_ok(got, ref, truth, floor, bar=1e-4):
+    """(ok, detail) for a Jacobi output compared per element."""
+    g_ref = elemstats(got, ref, floor)
+    if g_ref[0] < bar:
+        return True, {"vs_ref": g_ref}
+    g_truth = elemstats(got, truth, floor)
+    r_truth = elemstats(ref, truth, floor)
+    return g_truth[0] <= NOISE * r_truth[0], {"vs_ref": g_ref, "vs_fp64": g_truth, "ref_vs_fp64": r_truth}

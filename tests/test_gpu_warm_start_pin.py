@@ -5,7 +5,7 @@ The solve's first iterate replaces the reference's init_pressure
 (IISPH.py:166-174).  Checked here, per element, through the C ABI
 (sph_get_features, sph_get_solve_start):
 
-  * the 10 network inputs the neighbour build computes, against
+  * the 11 network inputs the neighbour build computes, against
     oracle.mlp_oracle.warm_start_features restated from the FP32 oracle's
     terms of the same step (rho_adv, a_ii, d_ii, the neighbour lists): within
     1e-4 of max(|input|, its standard deviation in the shipped network), the
@@ -79,16 +79,18 @@ def test_learned_inputs_and_prediction_vs_oracle(oracle):
     capped_before = bool(sol.last_stats["flags"] & _lib.SPH_F_NOT_CONVERGED)
     sol.step()
     f_gpu, p0_gpu = _features_and_start(sol)
+    grid = np.zeros(9)
+    _lib.check(sol._ctx, sol._lib.sph_get_grid(sol._ctx, 0, _lib.ptr(grid)))
     sol.close()
 
     ref = _oracle_step(oracle, params, x, v, scene.boundary_x, psi, dt)
     f_ref = M.warm_start_features(ref, x, p_prev, scene.boundary_x, psi, kernel_tables(params)[0],
-                                  _consts(params), dt)
+                                  _consts(params), dt, grid)
     blob = load_blob()
-    sd = blob[10:20]
+    sd = blob[M.NF:2 * M.NF]
     assert np.array_equal(f_gpu[:, 4], f_ref[:, 4]) and np.array_equal(f_gpu[:, 9], f_ref[:, 9])
     worst = {}
-    for k in range(10):
+    for k in range(M.NF):
         err = np.abs(f_gpu[:, k].astype(np.float64) - f_ref[:, k]) / np.maximum(np.abs(f_ref[:, k]), sd[k])
         worst[k] = float(err.max())
     assert max(worst.values()) < FEATURE_TOL, worst

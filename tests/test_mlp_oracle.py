@@ -13,16 +13,16 @@ def test_bf16_rounding_matches_torch():
 
 
 def test_blob_layout():
-    assert M.NPARAMS == 4929 and M.BLOB == 4950
+    assert M.NPARAMS == 4993 and M.BLOB == 5016
     from warpsph_b200 import _lib
     from warpsph_b200.learned import init_blob
 
     rng = np.random.default_rng(1)
-    f = rng.normal(0, 1, (256, 10)).astype(np.float32)
+    f = rng.normal(0, 1, (256, M.NF)).astype(np.float32)
     t = rng.normal(0, 3, 256).astype(np.float32)
     blob = init_blob(f, t)
     assert blob.size == _lib.SPH_MLP_BLOB
     w = M.unpack(blob)
-    assert w["W1"].shape == (10, 64) and w["W2"].shape == (64, 64)
+    assert w["W1"].shape == (11, 64) and w["W2"].shape == (64, 64)
     loss, grad, y = M.loss_and_grad(blob, f, t)
     assert grad.size == M.NPARAMS and np.isfinite(loss)

@@ -4,7 +4,8 @@ runtime (tests/golden/make_golden.py).  No GPU needed."""
 import numpy as np
 import pytest
 
-from tests.helpers import csr_equal, golden_oracle_params, load_golden, normrel
+from tests.helpers import (csr_equal, elemstats, golden_oracle_params, golden_solver_params, jacobi_output_ok,
+                           load_golden, normrel, parity_floors)
 
 SCENES = ["ref_lattice", "dam_jitter", "compressed", "viscous"]
 
@@ -44,6 +45,21 @@ def test_steps_match_reference(oracle, name):
                                ("s", "s", 2e-5), ("Ap", "Ap", 2e-5), ("v", "v_out", 2e-5), ("x", "x_out", 1e-6)):
             assert normrel(r[key], G[pre + gkey]) < tol, (name, s, key, normrel(r[key], G[pre + gkey]))
         assert r["dt_next"] == float(G[pre + "dt_out"])
+        # per element: pre-solve terms to float32 summation order, the
+        # Jacobi outputs to the FP32 noise floor (tests.helpers.jacobi_output_ok)
+        fl = parity_floors(golden_solver_params(meta), float(G[pre + "dt_in"]))
+        for key in ("rho", "rho_adv", "v_adv", "d_ii", "a_ii"):
+            assert elemstats(r[key], G[pre + key], fl[key])[0] < 5e-6, (name, s, key)
+        assert elemstats(r["v"], G[pre + "v_out"], fl["v"])[0] < 1e-4, (name, s)
+        assert elemstats(r["x"], G[pre + "x_out"], fl["x"], x_like=True)[0] < 1e-4, (name, s)
+        if s == 0:
+            t = oracle.step(P, G[pre + "x_in"], G[pre + "v_in"], G["boundary_x"], None, G["boundary_phi"],
+                            float(G[pre + "dt_in"]), float(G[pre + "inv_dt_in"]),
+                            tables=oracle.kernel_tables(P, np.float64), precision="f64",
+                            fixed_iters=int(G[pre + "iterations"]))
+            for key in ("p", "s", "Ap"):
+                ok, detail = jacobi_output_ok(r[key], G[pre + key], t[key], fl[key])
+                assert ok, (name, key, detail)
 
 
 def test_fp64_truth_close_to_fp32(oracle):

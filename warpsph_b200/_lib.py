@@ -69,9 +69,9 @@ class SphMlpTrainConfig(ctypes.Structure):
                 ("seed", ctypes.c_uint32), ("device", ctypes.c_int32)]
 
 
-SPH_MLP_FEATURES = 10
-SPH_MLP_PARAMS = 4929
-SPH_MLP_BLOB = 4950
+SPH_MLP_FEATURES = 11
+SPH_MLP_PARAMS = 4993
+SPH_MLP_BLOB = 5016
 SPH_MLP_MAX_RISE = 0.5
 
 
@@ -132,6 +132,7 @@ SIGNATURES = {
     "sph_set_record_features": (ctypes.c_int, [_P, ctypes.c_int32]),
     "sph_get_features": (ctypes.c_int, [_P, _P, _P]),
     "sph_get_solve_start": (ctypes.c_int, [_P, _P]),
+    "sph_get_grid": (ctypes.c_int, [_P, ctypes.c_int32, _P]),
     "sph_mlp_train": (ctypes.c_int, [ctypes.POINTER(SphMlpTrainConfig), _P, _P, ctypes.c_int64, _P, _P]),
     "sph_mlp_eval": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, ctypes.c_int32, _P, _P]),
     "sph_boundary_psi_noalloc": (ctypes.c_int, [ctypes.POINTER(SphParams), _P, ctypes.c_int64, _P, _P, _P]),

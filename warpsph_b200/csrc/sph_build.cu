@@ -273,6 +273,11 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Ker& ker) {
       f[7] = asinhf(p1 * p_ref);                               // Jacobi source term
       f[8] = gy * c.h * inv_rho0;                              // grad rho along gravity
       f[9] = float(cntb);                                      // boundary neighbour count
+      // hydrostatic pressure of the fluid column above: depth below the
+      // highest fluid particle of this grid column (x, z), in units of h
+      const int3 top = make_int3(ci.x, 0, ci.z);
+      const float depth = key_float(__ldg(a.coltop + fr.base + cell_index(g, top))) - xi.y;
+      f[10] = asinhf(fmaxf(depth, 0.f) / c.h);
     }
   }
   // bookkeeping: overflow flags, pair totals, max counts (once per step)
@@ -290,6 +295,25 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Ker& ker) {
     atomicMax(&a.acc->max_fb, mb);
     if (over) atomicOr(&a.acc->flags, over);
   }
+}
+
+// Highest fluid y of each grid column (x, z): every sorted fluid particle
+// raises the key of its column's bottom cell (cy = 0).
+__global__ void k_column_top(BuildArgs a, unsigned int* coltop) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const CellFrame fr = frame_of(a.scenes, a.grid, false, i);
+  const float4 xi = a.pos[i];
+  int3 c = cell_coord(fr.g, xi.x, xi.y, xi.z);
+  c.y = 0;
+  atomicMax(coltop + fr.base + cell_index(fr.g, c), float_key(xi.y));
+}
+
+cudaError_t launch_column_top(const BuildArgs& a, unsigned int* coltop, int total_cells, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(coltop, 0, sizeof(unsigned int) * size_t(total_cells), s);
+  if (e != cudaSuccess || a.n <= 0) return e;
+  k_column_top<<<(a.n + 255) / 256, 256, 0, s>>>(a, coltop);
+  return cudaGetLastError();
 }
 
 // predict_v_adv with viscosity (IISPH.py:217-278), after kBuildLists wrote

@@ -65,6 +65,7 @@ struct SphCtx {
   float *p_s = nullptr, *pprev_w = nullptr;
   int *key = nullptr, *rank = nullptr, *sort_src = nullptr, *sort_orig = nullptr;
   int *cell_count = nullptr, *cell_start = nullptr, *scan_part = nullptr;
+  unsigned int* coltop = nullptr;  // per grid column, the highest fluid y (warm-start input 10)
   int *nbr_ff = nullptr, *cnt_ff = nullptr, *nbr_fb = nullptr, *cnt_fb = nullptr;
   float* rho = nullptr;
   float4 *bvec = nullptr, *dii_aii = nullptr, *vadv = nullptr, *a4 = nullptr;
@@ -83,6 +84,8 @@ struct SphCtx {
   int blocks_per_sm = 0;
   size_t jac_smem = 0;
   int jac_block = 256, jac_ppt = 1, jac_unroll = 4;  // autotuner knobs of the solve
+  bool jac_tex = false;                               // pass B reads x_j through the texture path
+  cudaTextureObject_t pos_tex = 0;                    // over pos_w, when jac_tex
   int stall_block = -1;                               // sph_test_stall_barrier
   int withhold_mma = 0;                               // sph_test_withhold_mma
   int chunk = 256;                                    // particles per solve chunk
@@ -329,6 +332,7 @@ int set_grid(SphCtx* ctx, const float* xf, int64_t n) {
     CK(dalloc(ctx->cell_start, ctx->total_cells + 1));
     CK(dalloc(ctx->bcell_start, ctx->total_cells + 1));
     CK(dalloc(ctx->scan_part, ctx->total_cells / 4096 + 2));
+    CK(dalloc(ctx->coltop, ctx->total_cells));
     ctx->ncells_cap = ctx->total_cells;
   }
   int rc = upload_scene_table(ctx);
@@ -451,6 +455,24 @@ int alloc_neighbors(SphCtx* ctx) {
   return SPH_OK;
 }
 
+// A 1-D texture object over the solve's position array (float4 per slot).
+int make_pos_texture(SphCtx* ctx) {
+  if (ctx->pos_tex) {
+    cudaDestroyTextureObject(ctx->pos_tex);
+    ctx->pos_tex = 0;
+  }
+  if (!ctx->jac_tex) return SPH_OK;
+  cudaResourceDesc rd{};
+  rd.resType = cudaResourceTypeLinear;
+  rd.res.linear.devPtr = ctx->pos_w;
+  rd.res.linear.desc = cudaCreateChannelDesc<float4>();
+  rd.res.linear.sizeInBytes = sizeof(float4) * size_t(ctx->n_cap);
+  cudaTextureDesc td{};
+  td.readMode = cudaReadModeElementType;
+  CK(cudaCreateTextureObject(&ctx->pos_tex, &rd, &td, nullptr));
+  return SPH_OK;
+}
+
 int alloc_fluid(SphCtx* ctx, int64_t n) {
   if (n <= ctx->n_cap && ctx->pos_s) return SPH_OK;
   const int64_t m = std::max<int64_t>(n, 1);
@@ -458,6 +480,10 @@ int alloc_fluid(SphCtx* ctx, int64_t n) {
   CK(dalloc(ctx->pos_s, m));
   CK(dalloc(ctx->vel_s, m));
   CK(dalloc(ctx->pos_w, m));
+  {
+    const int rc = make_pos_texture(ctx);
+    if (rc) return rc;
+  }
   CK(dalloc(ctx->vel_w, m));
   CK(dalloc(ctx->orig_s, m));
   CK(dalloc(ctx->orig_w, m));
@@ -541,6 +567,7 @@ sph::BuildArgs build_args(SphCtx* ctx) {
   b.p0 = ctx->p_a;
   b.pos_q = ctx->pos_w;
   b.feat = (ctx->record_feat || ctx->P.warm_start == SPH_WARM_MLP) ? ctx->feat : nullptr;
+  b.coltop = ctx->coltop;
   return b;
 }
 
@@ -556,6 +583,7 @@ int enqueue_front(SphCtx* ctx) {
                         ctx->vel_w, ctx->orig_w, ctx->pprev_w, ctx->stream));
   int block = ctx->P.block_size > 0 ? ctx->P.block_size : 128;
   const sph::BuildArgs b = build_args(ctx);
+  if (b.feat) CK(sph::launch_column_top(b, ctx->coltop, ctx->total_cells, ctx->stream));
   if (ctx->P.vis_mu == 0.0) {
     CK(sph::launch_build(b, block, sph::kBuildFull, ctx->stream));
   } else {
@@ -637,6 +665,7 @@ int enqueue_jacobi(SphCtx* ctx) {
   // 0.5 p_prev start runs the reference's extra Ap_0 evaluation (pass 0).
   j.start_iter = (ctx->P.warm_start == SPH_WARM_HALF) ? 0 : 1;
   j.grad_spline = ctx->g_spline ? 1 : 0;
+  j.xtex = (ctx->jac_tex && ctx->g_spline) ? (unsigned long long)ctx->pos_tex : 0ull;
   j.budget = (long long)ctx->P.timeout_ms * (long long)ctx->clock_khz;
   j.stall_block = ctx->stall_block;
   j.dt_max = ctx->P.dt_max;
@@ -837,8 +866,12 @@ int sph_create(const SphParams* params, SphCtx** out) {
   ctx->jac_unroll = P.jacobi_unroll ? P.jacobi_unroll : 4;
   if (!sph::jacobi_variant_ok(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll)) return bail(SPH_E_INVALID);
   ctx->chunk = ctx->jac_block * ctx->jac_ppt;
+  {
+    const char* e = std::getenv("WPSPH_JACOBI_TEX");
+    ctx->jac_tex = e && e[0] == '1';
+  }
   if (sph::jacobi_config(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll, ctx->c.sg, ctx->g_spline, &ctx->blocks_per_sm,
-                         &ctx->jac_smem) != cudaSuccess ||
+                         &ctx->jac_smem, ctx->jac_tex) != cudaSuccess ||
       ctx->blocks_per_sm < 1)
     return bail(SPH_E_CUDA);
   ctx->coop_grid = ctx->blocks_per_sm * ctx->sm_count;
@@ -851,10 +884,11 @@ void sph_destroy(SphCtx* ctx) {
   cudaSetDevice(ctx->dev);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  if (ctx->pos_tex) cudaDestroyTextureObject(ctx->pos_tex);
   void* ptrs[] = {ctx->d_w, ctx->d_g, ctx->bpos, ctx->bvel, ctx->borig, ctx->bpos_t, ctx->bvel_t, ctx->borig_t,
                   ctx->bkey, ctx->brank, ctx->bsrc, ctx->bcell_start, ctx->pos_s, ctx->vel_s,
                   ctx->pos_w, ctx->vel_w, ctx->orig_s, ctx->orig_w, ctx->p_s, ctx->pprev_w, ctx->key, ctx->rank,
-                  ctx->sort_src, ctx->sort_orig, ctx->cell_count, ctx->cell_start, ctx->scan_part, ctx->nbr_ff,
+                  ctx->sort_src, ctx->sort_orig, ctx->cell_count, ctx->cell_start, ctx->scan_part, ctx->coltop, ctx->nbr_ff,
                   ctx->cnt_ff, ctx->nbr_fb, ctx->cnt_fb, ctx->rho, ctx->bvec, ctx->dii_aii, ctx->vadv, ctx->a4,
                   ctx->p_a, ctx->p_b, ctx->Ap, ctx->pmlp, ctx->feat, ctx->p_start, ctx->mlp, ctx->stage, ctx->partials, ctx->st, ctx->acc, ctx->ring,
                   ctx->d_scenes, ctx->d_chunks, ctx->d_chunk_scene,
@@ -888,7 +922,7 @@ int sph_set_tables(SphCtx* ctx, const float* w, int32_t nw, const float* g, int3
   if (rc) return rc;
   int b = 0;
   CK(sph::jacobi_config(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll, ctx->c.sg, ctx->g_spline, &b,
-                        &ctx->jac_smem));
+                        &ctx->jac_smem, ctx->jac_tex));
   if (b < 1) return fail(ctx, SPH_E_CUDA, "jacobi kernel does not fit");
   if (b != ctx->blocks_per_sm) {
     ctx->blocks_per_sm = b;
@@ -1479,6 +1513,16 @@ int sph_get_solve_start(SphCtx* ctx, float* p) {
   CK(cudaMemcpy(ow.data(), ctx->orig_w, sizeof(int) * n, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(h.data(), ctx->p_start, sizeof(float) * n, cudaMemcpyDeviceToHost));
   for (int64_t k = 0; k < n; ++k) p[ow[k]] = h[k];
+  return SPH_OK;
+}
+
+int sph_get_grid(SphCtx* ctx, int32_t scene, double* out) {
+  if (!ctx || !out || scene < 0 || scene >= ctx->S) return fail(ctx, SPH_E_INVALID, "bad scene or output");
+  if (!ctx->grid_valid) return fail(ctx, SPH_E_INVALID, "no grid yet: set the particles first");
+  const Grid& g = ctx->grids[scene];
+  const double v[9] = {g.ox, g.oy, g.oz, g.inv_cell, g.inv_cell_x, double(g.nx), double(g.ny), double(g.nz),
+                       double(ctx->cell_base[scene])};
+  for (int k = 0; k < 9; ++k) out[k] = v[k];
   return SPH_OK;
 }
 

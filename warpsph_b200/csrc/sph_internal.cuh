@@ -19,7 +19,7 @@
 namespace sph {
 
 constexpr int kWarp = 32;
-constexpr int kFeatures = 10;  // learned warm-start inputs per particle
+constexpr int kFeatures = 11;  // learned warm-start inputs per particle
 
 // Uniform neighbour grid.  Cell size is slightly above h (cell = 1.01 h or
 // coarser) in y and z; along x, the direction in which sorted rows run, cells
@@ -391,8 +391,19 @@ struct BuildArgs {
   float4* vadv;
   float* p0;               // initial pressure of the solve (p_1 for the zero warm start)
   float4* pos_q;           // the array `pos` points to: p0 / rho^2 goes into .w
-  float* feat;             // optional MLP feature rows (n x 10), NULL to skip
+  float* feat;             // optional MLP feature rows (n x kFeatures), NULL to skip
+  const unsigned int* coltop;  // with feat: per grid column (x, z), the highest fluid y (ordered key)
 };
+
+// Order-preserving uint key of a float (atomicMax on keys = max on floats);
+// key 0 is below every float's key.
+__device__ __forceinline__ unsigned int float_key(float y) {
+  const unsigned int u = __float_as_uint(y);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(unsigned int k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
 
 struct JacobiArgs {
   int n;
@@ -429,6 +440,7 @@ struct JacobiArgs {
   float* p_out;
   int start_iter;          // 1: p_1 came from the build; 0: warm start, run pass 0
   int grad_spline;         // 1: the gradient table is the cubic spline's (closed form in the passes)
+  unsigned long long xtex; // texture object over pos (0: none): pass B fetches x_j through the texture path
   long long budget;        // barrier spin budget in SM cycles
   int stall_block;         // test hook: this block skips its first barrier arrival (-1: none)
   double dt_max, cfl_len, inv_small_d, eta_d;
@@ -452,13 +464,16 @@ cudaError_t launch_sort(const SortArgs& a, int ncells, cudaStream_t s);
 constexpr int kBuildFull = 0, kBuildLists = 1, kBuildAdvect = 2;
 cudaError_t launch_build(const BuildArgs& a, int block, int mode, cudaStream_t s);
 cudaError_t launch_visc(const BuildArgs& a, int block, cudaStream_t s);
+// highest fluid y of every grid column (x, z) into a.coltop (zeroed first)
+cudaError_t launch_column_top(const BuildArgs& a, unsigned int* coltop, int total_cells, cudaStream_t s);
 cudaError_t launch_psi(const PsiArgs& a, int block, cudaStream_t s);
 cudaError_t launch_psi_sorted(const PsiArgs& a, float* psi_sorted, int block, cudaStream_t s);
 cudaError_t launch_gather(int n, const int* sort_src, const int* sort_orig, const float4* pos_in,
                           const float4* vel_in, const float* p_in, float4* pos_out, float4* vel_out,
                           int* orig_out, float* p_out, cudaStream_t s);
 bool jacobi_variant_ok(int block, int ppt, int unroll);
-cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, bool spline, int* blocks_per_sm, size_t* smem);
+cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, bool spline, int* blocks_per_sm, size_t* smem,
+                          bool tex = false);
 cudaError_t launch_jacobi(const JacobiArgs& a, int grid, int block, int ppt, int unroll, size_t smem,
                           cudaStream_t s);
 cudaError_t launch_pack_fluid(int n, int base, const float* x3, const float* v3, float4* pos, float4* vel,

@@ -52,9 +52,19 @@ namespace sph {
 // resident instead of the list stream.  pos (its .w) and a4 are rewritten
 // between barriers, so they are read with plain coherent loads.  NG = 1
 // gathers pos only, NG = 2 also the second array.
-template <int kUnroll, int NG, typename Body>
+// Positions of neighbours: plain coherent loads, or (XT) fetches through the
+// texture path from a texture object over the same array, which only pass B
+// uses (it reads x_j, which the solve never changes, and not .w).
+template <bool XT>
+__device__ __forceinline__ float4 load_pos(const float4* pos, unsigned long long tex, int j) {
+  if (XT) return tex1Dfetch<float4>(cudaTextureObject_t(tex), j);
+  return pos[j];
+}
+
+template <int kUnroll, int NG, bool XT = false, typename Body>
 __device__ __forceinline__ void for_neighbours(const int* __restrict__ nb, int cnt, int self,
-                                               const float4* pos, const float4* other, Body body) {
+                                               const float4* pos, const float4* other, Body body,
+                                               unsigned long long xtex = 0) {
   const int wmax = __reduce_max_sync(0xffffffffu, cnt);
   int jn[kUnroll];
 #pragma unroll
@@ -70,7 +80,7 @@ __device__ __forceinline__ void for_neighbours(const int* __restrict__ nb, int c
     float4 xj[kUnroll], oj[kUnroll];
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
-      xj[u] = pos[j[u]];
+      xj[u] = load_pos<XT>(pos, xtex, j[u]);
       if (NG == 2) oj[u] = other[j[u]];
     }
 #pragma unroll
@@ -105,7 +115,7 @@ __device__ inline void pass_a(int i, bool live, const JacobiArgs& a, const Tab& 
 
 // pass B for particle i: Ap (compute_term_Ap_2, IISPH.py:469-518), the density
 // error (update_rho_error, IISPH.py:542-567) and p_{k+1} (update_p, IISPH.py:521-539)
-template <int U, class Tab>
+template <int U, bool XT, class Tab>
 __device__ inline void pass_b(int i, bool live, const JacobiArgs& a, const Tab& G, const float* pc, float* pn,
                               double& es, long long& ec) {
   const Consts& c = a.c;
@@ -114,11 +124,11 @@ __device__ inline void pass_b(int i, bool live, const JacobiArgs& a, const Tab& 
   const int cnt = live ? min(__ldg(a.cnt_ff + i), c.max_ff) : 0;
   const int* nb = a.nbr_ff + ell_index(i, 0, c.max_ff);
   float acc = 0.f;
-  for_neighbours<U, 2>(nb, cnt, i, a.pos, a.a4, [&](const float4 xj, const float4 aj) {
+  for_neighbours<U, 2, XT>(nb, cnt, i, a.pos, a.a4, [&](const float4 xj, const float4 aj) {
     const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
     const float gs = G(c, dx * dx + dy * dy + dz * dz);
     acc = fmaf(gs, (ai.x - aj.x) * dx + (ai.y - aj.y) * dy + (ai.z - aj.z) * dz, acc);
-  });
+  }, a.xtex);
   if (!live) return;
   const float4 bv = __ldg(a.bvec + i);
   const float4 da = __ldg(a.dii_aii + i);
@@ -140,12 +150,13 @@ __device__ inline void pass_b(int i, bool live, const JacobiArgs& a, const Tab& 
   a.Ap[i] = Ap;
 }
 
-template <int T, int PPT, int U, class Tab>
+template <int T, int PPT, int U, bool XT, class Tab>
 __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G);
 
 // How the passes get the kernel gradient: the table staged in shared memory,
-// the table in global memory (too large to stage), or the closed form.
-constexpr int kGradSmem = 0, kGradFlat = 1, kGradSpline = 2;
+// the table in global memory (too large to stage), or the closed form; the
+// last also with pass B's position gathers through the texture path.
+constexpr int kGradSmem = 0, kGradFlat = 1, kGradSpline = 2, kGradSplineTex = 3;
 
 // GM gradient mode, T threads per block, PPT particles per thread (chunks of
 // T * PPT particles), neighbour-loop unroll U: the knobs the autotuner chooses among.
@@ -154,11 +165,11 @@ __global__ void __launch_bounds__(T) k_jacobi(JacobiArgs a) {
   extern __shared__ float2 s_pairs[];
   if (GM == kGradSmem) {
     stage_slopes(s_pairs, a.g_table, a.c.sg);
-    jacobi_body<T, PPT, U>(a, TableGrad<SlopeTable>{SlopeTable{s_pairs}});
+    jacobi_body<T, PPT, U, false>(a, TableGrad<SlopeTable>{SlopeTable{s_pairs}});
   } else if (GM == kGradFlat) {
-    jacobi_body<T, PPT, U>(a, TableGrad<FlatSlopeTable>{FlatSlopeTable{a.g_table}});
+    jacobi_body<T, PPT, U, false>(a, TableGrad<FlatSlopeTable>{FlatSlopeTable{a.g_table}});
   } else {
-    jacobi_body<T, PPT, U>(a, SplineGrad{});
+    jacobi_body<T, PPT, U, GM == kGradSplineTex>(a, SplineGrad{});
   }
 }
 
@@ -186,7 +197,7 @@ __device__ __forceinline__ void block_sum2(double& v, long long& c, double* sv, 
   __syncthreads();
 }
 
-template <int T, int PPT, int U, class Tab>
+template <int T, int PPT, int U, bool XT, class Tab>
 __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G) {
   __shared__ double s_sum[T / 32];
   __shared__ long long s_cnt[T / 32];
@@ -256,7 +267,7 @@ __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G) {
 #pragma unroll
         for (int q = 0; q < PPT; ++q) {
           const int i = r.x + q * T + threadIdx.x;
-          pass_b<U>(i < r.y ? i : r.x, i < r.y, a, G, pc, pn, es, ec);
+          pass_b<U, XT>(i < r.y ? i : r.x, i < r.y, a, G, pc, pn, es, ec);
         }
       }
       if (run >= 0) flush();
@@ -461,8 +472,8 @@ __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G) {
   }
 }
 
-static int grad_mode(int sg, bool spline) {
-  return spline ? kGradSpline : (sg <= 8192 ? kGradSmem : kGradFlat);
+static int grad_mode(int sg, bool spline, bool tex = false) {
+  return spline ? (tex ? kGradSplineTex : kGradSpline) : (sg <= 8192 ? kGradSmem : kGradFlat);
 }
 static size_t jacobi_smem(int mode, int sg) { return mode == kGradSmem ? sizeof(float2) * size_t(sg) : 0; }
 
@@ -492,6 +503,7 @@ static JacobiKernel jacobi_kernel(int mode, int T, int ppt, int unroll) {
   switch (mode) {
     case kGradSmem: return pick_jacobi<kGradSmem>(T, ppt, unroll);
     case kGradFlat: return pick_jacobi<kGradFlat>(T, ppt, unroll);
+    case kGradSplineTex: return pick_jacobi<kGradSplineTex>(T, ppt, unroll);
     default: return pick_jacobi<kGradSpline>(T, ppt, unroll);
   }
 }
@@ -500,8 +512,9 @@ bool jacobi_variant_ok(int block, int ppt, int unroll) {
   return pick_jacobi<kGradSpline>(block, ppt, unroll) != nullptr;
 }
 
-cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, bool spline, int* blocks_per_sm, size_t* smem_out) {
-  const int mode = grad_mode(sg, spline);
+cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, bool spline, int* blocks_per_sm, size_t* smem_out,
+                          bool tex) {
+  const int mode = grad_mode(sg, spline, tex);
   JacobiKernel k = jacobi_kernel(mode, block, ppt, unroll);
   if (!k) return cudaErrorInvalidValue;
   const size_t smem = jacobi_smem(mode, sg);
@@ -519,7 +532,7 @@ cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, bool spline, i
 
 cudaError_t launch_jacobi(const JacobiArgs& a, int grid, int block, int ppt, int unroll, size_t smem,
                           cudaStream_t s) {
-  JacobiKernel k = jacobi_kernel(grad_mode(a.c.sg, a.grad_spline != 0), block, ppt, unroll);
+  JacobiKernel k = jacobi_kernel(grad_mode(a.c.sg, a.grad_spline != 0, a.xtex != 0), block, ppt, unroll);
   if (!k) return cudaErrorInvalidValue;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);

@@ -17,7 +17,7 @@ constexpr int kW1Pitch = 24;  // row pitch (bf16) of w1f: 8 rows hit 8 distinct 
 constexpr int kWPitch = 72;   // row pitch (bf16) of the 64-wide matrices
 
 // Parameter order inside the FP32 blob's parameter block and the gradient
-// vector (SPH_MLP_* in include/wpsph.h):  W1 [10][64] (in, out), b1 [64],
+// vector (SPH_MLP_* in include/wpsph.h):  W1 [11][64] (in, out), b1 [64],
 // W2 [64][64] (in, out), b2 [64], w3 [64], b3.
 constexpr int kOffW1 = 0;
 constexpr int kOffB1 = kOffW1 + kFeatures * kH;
@@ -25,15 +25,15 @@ constexpr int kOffW2 = kOffB1 + kH;
 constexpr int kOffB2 = kOffW2 + kH * kH;
 constexpr int kOffW3 = kOffB2 + kH;
 constexpr int kOffB3 = kOffW3 + kH;
-constexpr int kNumParams = kOffB3 + 1;  // 4929
+constexpr int kNumParams = kOffB3 + 1;  // 4993
 constexpr int kOffLoss = kNumParams;    // gradient vector slot holding the loss
 constexpr int kGradStride = kNumParams + 3;
-// FP32 blob: mu[10], sd[10], t_scale, then the parameters.
+// FP32 blob: mu[11], sd[11], t_scale, then the parameters.
 constexpr int kBlobMu = 0;
 constexpr int kBlobSd = kBlobMu + kFeatures;
 constexpr int kBlobTScale = kBlobSd + kFeatures;
 constexpr int kBlobParams = kBlobTScale + 1;
-constexpr int kBlobSize = kBlobParams + kNumParams;  // 4950
+constexpr int kBlobSize = kBlobParams + kNumParams;  // 5016
 
 // Weights as the kernels read them (bf16 matrices in fragment-friendly layouts).
 struct MlpPacked {

@@ -220,7 +220,9 @@ __global__ void __launch_bounds__(kTile) k_mlp_infer_tc(MlpInferArgs a) {
   for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const long long row = tile * kTile + tid;
     const bool live = row < a.n;
-    const float u_prev = fn[3];  // asinh(p_prev / (rho0 g h)), the residual's base, unrounded
+    // the residual's base, unrounded: the larger of asinh(p_prev / (rho0 g h))
+    // and asinh(depth / h), the hydrostatic pressure of the column above
+    const float u_prev = fmaxf(fn[3], fn[10]);
     // 1. standardised features of this row, BF16, K padded to 16 with zeros
     {
       float f[kIn];

@@ -1,15 +1,16 @@
 """Learned pressure warm start: data collection, training and storage.
 
-The network (10 -> 64 -> 64 -> 1, BF16 tensor cores) is trained on the
+The network (11 -> 64 -> 64 -> 1, BF16 tensor cores) is trained on the
 solver's own converged pressures: every step of a set of dam-break scenes
-exports each particle's 10 inputs and asinh(p / (rho0 g h)) of its converged
+exports each particle's 11 inputs and asinh(p / (rho0 g h)) of its converged
 pressure (sph_get_features), a sample of them forms the training set, and
 sph_mlp_train fits the network on the GPU (Adam, MSE).  The network is
-residual: it predicts the change of asinh(p / (rho0 g h)) from the previous
-step's value (input 3), which the inference kernel adds back in float32, so
-the network's BF16 arithmetic only touches the small correction.  At run time
-SPH_WARM_MLP starts the relaxed Jacobi solve from the prediction; the solve's
-stopping rule is unchanged.
+residual: it predicts the change of asinh(p / (rho0 g h)) from a base, the
+larger of the previous step's value (input 3) and the hydrostatic pressure of
+the fluid column above the particle (input 10), which the inference kernel
+adds back in float32, so the network's BF16 arithmetic only touches the
+correction.  At run time SPH_WARM_MLP starts the relaxed Jacobi solve from the
+prediction; the solve's stopping rule is unchanged.
 
 Inputs (computed in the neighbour build, all dimensionless):
  0 rho_adv / rho0 - 1            predicted density deviation
@@ -22,6 +23,9 @@ Inputs (computed in the neighbour build, all dimensionless):
  7 asinh(p_1 / (rho0 g h))       first Jacobi iterate from p = 0
  8 (grad rho)_y h / rho0         density gradient along gravity
  9 boundary neighbour count
+10 asinh(depth / h)              hydrostatic pressure of the fluid column above:
+                                 depth below the highest fluid particle of the
+                                 particle's neighbour-grid column (x, z)
 """
 
 from __future__ import annotations
@@ -54,12 +58,18 @@ def init_blob(feat: np.ndarray, target: np.ndarray, seed: int = 0) -> np.ndarray
     return blob
 
 
-SKIP = 3  # input carried around the network: asinh(p_prev / (rho0 g h))
+PREV, HYDRO = 3, 10  # inputs whose larger value is carried around the network
+
+
+def base(feat) -> np.ndarray:
+    """The residual's base: max(asinh(p_prev / (rho0 g h)), asinh(depth / h))."""
+    f = np.asarray(feat, np.float32)
+    return np.maximum(f[:, PREV], f[:, HYDRO])
 
 
 def residual_target(feat, target) -> np.ndarray:
-    """What the network regresses: the target minus the skip input."""
-    return (np.asarray(target, np.float32) - np.asarray(feat, np.float32)[:, SKIP]).astype(np.float32)
+    """What the network regresses: the target minus the base."""
+    return (np.asarray(target, np.float32) - base(feat)).astype(np.float32)
 
 
 def train(feat, target, epochs=20, batch=4096, lr=1e-3, seed=0, device=0, blob=None):
@@ -78,11 +88,11 @@ def train(feat, target, epochs=20, batch=4096, lr=1e-3, seed=0, device=0, blob=N
 
 
 def predict(blob, feat, device=0) -> np.ndarray:
-    """Predicted asinh(p / (rho0 g h)) before the clamp at 0: the skip input
-    plus the network's correction, whose rise is bounded by SPH_MLP_MAX_RISE."""
+    """Predicted asinh(p / (rho0 g h)) before the clamp at 0: the base plus
+    the network's correction, whose rise is bounded by SPH_MLP_MAX_RISE."""
     feat = np.ascontiguousarray(feat, np.float32)
     y = evaluate(blob, feat, device=device)
-    return feat[:, SKIP] + np.minimum(y * np.float32(blob[2 * NF]), np.float32(_lib.SPH_MLP_MAX_RISE))
+    return base(feat) + np.minimum(y * np.float32(blob[2 * NF]), np.float32(_lib.SPH_MLP_MAX_RISE))
 
 
 def evaluate(blob, feat, target=None, device=0):
@@ -104,11 +114,12 @@ def evaluate(blob, feat, target=None, device=0):
     return pred, float(grad[-1]), grad[:-1]
 
 
-def collect(scenes, steps, per_step, params_for, seed=0, warm="half", skip=0):
+def collect(scenes, steps, per_step, params_for, seed=0, warm="zero", skip=0, skip_capped=True):
     """Run each scene for ``steps`` steps, sampling ``per_step`` (input, target)
-    pairs per step after the first ``skip`` steps (the start-up transient,
-    whose pressure jumps would dominate a mean-squared loss).
-    ``params_for(scene)`` gives the SolverParams."""
+    pairs per step after the first ``skip`` steps.  With ``skip_capped``,
+    steps whose solve stopped at the iteration cap are left out: their
+    pressure is not a solution of the step's system.  ``params_for(scene)``
+    gives the SolverParams."""
     from .solver import IISPH
 
     rng = np.random.default_rng(seed)
@@ -121,7 +132,7 @@ def collect(scenes, steps, per_step, params_for, seed=0, warm="half", skip=0):
         t = np.zeros(n, np.float32)
         for k in range(steps):
             sol.step()
-            if k < skip:
+            if k < skip or (skip_capped and sol.last_stats["flags"] & _lib.SPH_F_NOT_CONVERGED):
                 continue
             _lib.check(sol._ctx, sol._lib.sph_get_features(sol._ctx, _lib.ptr(f), _lib.ptr(t)))
             pick = rng.choice(n, size=min(per_step, n), replace=False)

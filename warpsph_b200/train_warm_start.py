@@ -5,16 +5,17 @@
 Data: the solver's own converged pressures on the 64 batched dam-break scenes
 (`scenes.batched_scenes`, 0.01 m spacing, dt 5e-4, 1024-sample tables,
 g = 9.81), `--steps` steps each, sampled evenly to `--pairs` pairs after each
-scene's first `--skip` steps.  Training: Adam, lr 1e-3, MSE, on the GPU with
+scene's first `--skip` steps (default none: the start-up transient is in the
+data), leaving out steps whose solve stopped at the iteration cap (their
+pressure solves nothing).  Training: Adam, lr 1e-3, MSE, on the GPU with
 libwpsph's own kernels.
 
-The first fit uses data from runs started at 0.5 p_prev.  Those runs fling
-separating particles (that start over-predicts pressure where the stopping
-test does not look), so their states are not the ones the network meets.
-Each of `--rounds` further rounds therefore collects with the previous
-network as the warm start, the states the shipped solver visits, and fits a
-fresh network to that data resampled with weight 1 + alpha * max(target, 0)
-(`learned.weighted_resample`).  Output: warpsph_b200/data/warm_start_mlp.npz.
+The first fit uses data from the reference's own runs (p = 0 start).  Each of
+`--rounds` further rounds collects with the previous network as the warm
+start, the states the shipped solver visits (its first steps converge, where
+the p = 0 runs hit the cap), and fits a fresh network to that data resampled
+with weight 1 + alpha * max(target, 0) (`learned.weighted_resample`).
+Output: warpsph_b200/data/warm_start_mlp.npz.
 """
 
 from __future__ import annotations
@@ -39,7 +40,7 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--out", default=str(learned.DEFAULT_WEIGHTS))
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--skip", type=int, default=20, help="start-up steps of each scene left out of the data")
+    ap.add_argument("--skip", type=int, default=0, help="start-up steps of each scene left out of the data")
     ap.add_argument("--rounds", type=int, default=2, help="on-policy rounds after the first fit")
     ap.add_argument("--alpha", type=float, default=1.0, help="resampling weight 1 + alpha * max(target, 0)")
     a = ap.parse_args()
@@ -47,7 +48,8 @@ def main():
     per_step = max(1, a.pairs // (a.scenes * max(1, a.steps - a.skip)))
     t0 = time.time()
     params = SolverParams(diameter=0.01, gravity=9.81, w_table_size=1024, g_table_size=1024)
-    feat, target = learned.collect(scenes, a.steps, per_step, lambda sc: params, seed=a.seed, skip=a.skip)
+    feat, target = learned.collect(scenes, a.steps, per_step, lambda sc: params, seed=a.seed, warm="zero",
+                                   skip=a.skip)
     t_collect = time.time() - t0
     t1 = time.time()
     blob, losses = learned.train(feat, target, epochs=a.epochs, lr=a.lr, seed=a.seed)
