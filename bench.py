@@ -379,7 +379,7 @@ def bench_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = run_cpu_reference(budget_s=15.0, max_steps=K)
+        cpu = run_cpu_reference(budget_s=30.0, max_steps=K)
 
     if rank == 0:
         line = {
