@@ -4,8 +4,10 @@ Restates, in numpy, the forward pass and the gradient of the mean squared
 error that libwpsph's tensor-core kernels compute, with the same BF16 rounding
 points: standardised inputs, weights, hidden activations and the
 back-propagated layer-2/layer-1 deltas are rounded to bfloat16 (round to
-nearest even) before each product; sums are taken in float64 here (the GPU
-accumulates in FP32, which is the difference the tests tolerate).
+nearest even) before each product; sums are taken in float64 here (the
+training kernels accumulate in FP32, which is the difference the tests
+tolerate), or, for the step's tensor-core inference, as that kernel
+accumulates (``forward(..., tc=True)``).
 
 Blob layout (include/wpsph.h): mu[11], sd[11], t_scale, then W1[11][64],
 b1[64], W2[64][64], b2[64], w3[64], b3 with W[in][out].
@@ -44,15 +46,36 @@ def unpack(blob):
     return out
 
 
-def forward(blob, feat):
+def trunc32(a) -> np.ndarray:
+    """float64 values rounded toward zero to float32."""
+    a = np.asarray(a, np.float64)
+    b = a.astype(np.float32)
+    over = np.abs(b.astype(np.float64)) > np.abs(a)
+    b[over] = np.nextafter(b[over], np.float32(0))
+    return b
+
+
+def forward(blob, feat, tc=False):
+    """Forward pass.  tc=False: the products summed exactly (float64).
+    tc=True: as the step's tensor-core inference kernel accumulates, which
+    this restatement matches by taking each layer's exact dot product rounded
+    toward zero to float32 before the float32 bias add (measured: with the
+    float64 sums instead, single hidden units land on the other side of a
+    BF16 rounding boundary and the output moves by ~5e-4)."""
     w = unpack(blob)
     inv_sd = (np.float32(1.0) / w["sd"]).astype(np.float32)
     x = ((np.asarray(feat, np.float32) - w["mu"]) * inv_sd).astype(np.float32)
     xb = bf16(x).astype(np.float64)
     W1, W2, w3 = (bf16(w[k]).astype(np.float64) for k in ("W1", "W2", "w3"))
-    z1 = xb @ W1 + w["b1"]
+    if tc:
+        z1 = (trunc32(xb @ W1) + w["b1"]).astype(np.float64)
+    else:
+        z1 = xb @ W1 + w["b1"]
     h1 = bf16(np.maximum(z1, 0).astype(np.float32)).astype(np.float64)
-    z2 = h1 @ W2 + w["b2"]
+    if tc:
+        z2 = (trunc32(h1 @ W2) + w["b2"]).astype(np.float64)
+    else:
+        z2 = h1 @ W2 + w["b2"]
     h2 = bf16(np.maximum(z2, 0).astype(np.float32)).astype(np.float64)
     y = h2 @ w3 + w["b3"][0]
     return dict(xb=xb, z1=z1, h1=h1, z2=z2, h2=h2, y=y, W2=W2, w3=w3)
@@ -177,7 +200,7 @@ def solve_start(blob, feat, consts, max_rise=0.5):
     rise bounded by max_rise, clamped at 0 and mapped back:
     p = sinh(max(u + min(y t_scale, max_rise), 0)) rho0 g h."""
     feat = np.asarray(feat, np.float32)
-    y = forward(blob, feat)["y"].astype(np.float32)
+    y = forward(blob, feat, tc=True)["y"].astype(np.float32)
     ts = np.float32(unpack(blob)["t_scale"])
     u = np.maximum(feat[:, 3], feat[:, 10])
     p_unit = np.float32(float(consts["rho0"]) * float(consts["gravity"]) * float(consts["h"]))

@@ -11,7 +11,8 @@ in.  Bars, per element with the floors of tests.helpers.parity_floors:
     the reference's count supplies p, s, Ap, v and x;
   * every quantity within 1e-4 relative of the FP32 oracle (the maximum over
     elements), and the CFL dt within 1e-4 — except that the relaxed-Jacobi
-    outputs p, s and Ap may instead be no further from the FP64 oracle than
+    outputs p, s, Ap and v (v = v_adv + (d_ii p + s) / dt) may instead be no
+    further from the FP64 oracle than
     NOISE times the FP32 oracle's own distance from it: an FP32 evaluation of
     the reference's arithmetic in another summation order already moves
     single particles' pressures by ~5e-4 of their value (the solve divides
@@ -26,7 +27,7 @@ from tests.parity_table import QUANTITIES, StepChecker, merge, run_dam_break_1m
 pytestmark = pytest.mark.gpu
 
 BAR = 1e-4
-JACOBI_OUT = ("p", "s", "Ap")
+JACOBI_OUT = ("p", "s", "Ap", "v")
 
 
 def out_of_bar(cmp):

@@ -25,7 +25,9 @@ def test_forward_and_gradient_match_oracle():
     blob = learned.init_blob(f, t, seed=3)
     pred, loss, grad = learned.evaluate(blob, f, t)
     loss_o, grad_o, y_o = M.loss_and_grad(blob, f, t)
-    assert normrel(pred, y_o) < 1e-4
+    # the tensor-core inference against the oracle that accumulates as it does
+    assert normrel(pred, M.forward(blob, f, tc=True)["y"]) < 1e-5
+    assert normrel(pred, y_o) < 2e-3
     assert abs(loss - loss_o) < 1e-4 * loss_o
     assert normrel(grad, grad_o) < 1e-3
     # per-block: every parameter group agrees

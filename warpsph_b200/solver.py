@@ -109,9 +109,6 @@ class IISPH:
             self._set_scene(scene)
 
         self._create_context()
-        if rigid_v is not None:
-            # set_rigid_v at sim_time 0 (IISPH.py:1061-1081), before the first step
-            self.set_rigid_velocity(rigid_v)
 
         self.renderer = FrameRecorder(stage_path, self._fps) if stage_path else None
         if preview:
@@ -130,6 +127,9 @@ class IISPH:
         self.term_Ap_i = DeviceField(self, "Ap", 1, "n")
         self.boundary_x = DeviceField(self, "boundary_x", 3, "boundary_n")
         self.boundary_phi = DeviceField(self, "boundary_phi", 1, "boundary_n")
+        if rigid_v is not None:
+            # set_rigid_v at sim_time 0 (IISPH.py:1061-1081), before the first step
+            self.set_rigid_velocity(rigid_v)
 
     # ------------------------------------------------------------------ scene
 
