@@ -4,7 +4,7 @@ update_rigid_x and the per-step boundary grid rebuild, IISPH.py:651-671,
 import numpy as np
 import pytest
 
-from tests.helpers import csr_equal, normrel
+from tests.helpers import csr_equal, elemstats, jacobi_output_ok, parity_floors
 
 pytestmark = pytest.mark.gpu
 
@@ -46,10 +46,19 @@ def test_moving_paddle_matches_oracle_each_step(oracle):
         nb = sol.get_neighbors(with_boundary=True)
         assert csr_equal(nb["ff_off"], nb["ff_idx"], ref["ff_off"], ref["ff_idx"]), step
         assert csr_equal(nb["fb_off"], nb["fb_idx"], ref["fb_off"], ref["fb_idx"]), step
-        assert normrel(sol.rho_adv.numpy(), ref["rho_adv"]) < RTOL, step
+        fl = parity_floors(params, float(dt))
+        assert elemstats(sol.rho_adv.numpy(), ref["rho_adv"], fl["rho_adv"])[0] < RTOL, step
         assert abs(sol.last_stats["iterations"] - ref["iterations"]) <= 1
         if sol.last_stats["iterations"] == ref["iterations"]:
-            assert normrel(sol.x.numpy(), ref["x"]) < 1e-6
+            # per element; the moving boundary makes a fixed-iteration twin
+            # of this state awkward, and the counts agree on these steps
+            assert elemstats(sol.x.numpy(), ref["x"], fl["x"], x_like=True)[0] < RTOL, step
+            truth = oracle.step(op, x, v, bx, bv, psi, float(dt), 1.0 / float(dt),
+                                tables=oracle.kernel_tables(op, np.float64), precision="f64",
+                                fixed_iters=int(ref["iterations"]))
+            for k, got in (("p", sol.p.numpy()), ("v", sol.v.numpy())):
+                ok, detail = jacobi_output_ok(got, ref[k], truth[k], fl[k])
+                assert ok, (step, k, detail)
         # update_rigid_x: x_b += v_b dt in float32, walls unchanged
         moved = (bx + bv * dt).astype(np.float32)
         assert np.array_equal(sol.boundary_x.numpy(), moved), step

@@ -10,7 +10,7 @@ what its exported terms give."""
 import numpy as np
 import pytest
 
-from tests.helpers import csr_equal, normrel
+from tests.helpers import csr_equal, elemstats, jacobi_output_ok, parity_floors
 
 pytestmark = pytest.mark.gpu
 
@@ -46,17 +46,27 @@ def full_step(oracle):
                                  g_size=params.g_table_size)
     ref = oracle.step(op, x, v, scene.boundary_x, None, psi, dt, 1.0 / dt, tables=kernel_tables(params),
                       fixed_iters=FIXED)
-    return out, ref, params
+    truth = oracle.step(op, x, v, scene.boundary_x, None, psi, dt, 1.0 / dt, tables=oracle.kernel_tables(op, np.float64),
+                        precision="f64", fixed_iters=FIXED)
+    out["dt"] = dt
+    return out, (ref, truth), params
 
 
 def test_full_size_step_vs_oracle(full_step):
-    out, ref, _ = full_step
+    """Per element (tests.helpers): the terms before the solve within 1e-4 of
+    the FP32 oracle, p and v within 1e-4 or at the FP32 noise floor against
+    the FP64 oracle, x within 1e-4 of the spacing."""
+    out, (ref, truth), params = full_step
+    fl = parity_floors(params, out["dt"])
     assert out["stats"]["iterations"] == FIXED
     assert csr_equal(out["nb"]["ff_off"], out["nb"]["ff_idx"], ref["ff_off"], ref["ff_idx"])
     assert csr_equal(out["nb"]["fb_off"], out["nb"]["fb_idx"], ref["fb_off"], ref["fb_idx"])
-    for k in ("rho", "rho_adv", "a_ii", "p", "v"):
-        assert normrel(out[k], ref[k]) < RTOL, k
-    assert normrel(out["x"], ref["x"]) < 1e-6
+    for k in ("rho", "rho_adv", "a_ii"):
+        assert elemstats(out[k], ref[k], fl[k])[0] < RTOL, k
+    for k in ("p", "v"):
+        ok, detail = jacobi_output_ok(out[k], ref[k], truth[k], fl[k])
+        assert ok, (k, detail)
+    assert elemstats(out["x"], ref["x"], fl["x"], x_like=True)[0] < RTOL
 
 
 def test_full_size_neighbour_relation_symmetric(full_step):
@@ -143,10 +153,16 @@ def test_full_size_pour_step_vs_oracle(oracle):
     op = oracle.reference_params(diameter=params.diameter, gravity=params.gravity, w_size=params.w_table_size,
                                  g_size=params.g_table_size)
     ref = oracle.step(op, x, v, bx, None, psi, dt, 1.0 / dt, tables=kernel_tables(params), fixed_iters=FIXED)
+    truth = oracle.step(op, x, v, bx, None, psi, dt, 1.0 / dt, tables=oracle.kernel_tables(op, np.float64),
+                        precision="f64", fixed_iters=FIXED)
+    fl = parity_floors(params, dt)
     assert one.last_stats["iterations"] == FIXED
     assert csr_equal(nb["ff_off"], nb["ff_idx"], ref["ff_off"], ref["ff_idx"])
     assert csr_equal(nb["fb_off"], nb["fb_idx"], ref["fb_off"], ref["fb_idx"])
-    for k, got in (("rho", one.rho), ("rho_adv", one.rho_adv), ("p", one.p), ("v", one.v)):
-        assert normrel(got.numpy(), ref[k]) < RTOL, k
-    assert normrel(one.x.numpy(), ref["x"]) < 1e-6
+    for k, got in (("rho", one.rho), ("rho_adv", one.rho_adv)):
+        assert elemstats(got.numpy(), ref[k], fl[k])[0] < RTOL, k
+    for k, got in (("p", one.p), ("v", one.v)):
+        ok, detail = jacobi_output_ok(got.numpy(), ref[k], truth[k], fl[k])
+        assert ok, (k, detail)
+    assert elemstats(one.x.numpy(), ref["x"], fl["x"], x_like=True)[0] < RTOL
     one.close()

@@ -115,15 +115,55 @@ def test_golden_fixed_iterations(oracle, name):
         sol.close()
 
 
-def _oracle_step(oracle, params, x, v, bx, psi, dt, inv_dt, precision="f32", **kw):
+def _oracle_step(oracle, params, x, v, bx, psi, dt, inv_dt, precision="f32", tables=None, **kw):
     from warpsph_b200.tables import kernel_tables
 
     op = oracle.reference_params(diameter=params.diameter, gravity=params.gravity, w_size=params.w_table_size,
                                  g_size=params.g_table_size, vis_mu_scale=params.vis_mu_scale)
-    tabs = kernel_tables(params)
+    tabs = kernel_tables(params) if tables is None else tables
     if precision == "f64":
-        tabs = oracle.kernel_tables(op, np.float64)
+        tabs = oracle.kernel_tables(op, np.float64) if tables is None else tuple(np.float64(t) for t in tables)
     return oracle.step(op, x, v, bx, None, psi, dt, inv_dt, tables=tabs, precision=precision, **kw)
+
+
+_FIELDS = {"rho": "rho", "rho_adv": "rho_adv", "v_adv": "v_adv", "d_ii": "term_d_ii", "a_ii": "term_a_ii",
+           "s": "sum_d_ij_p_j", "Ap": "term_Ap_i", "p": "p", "v": "v", "x": "x"}
+_JACOBI = ("p", "s", "Ap", "v")
+
+
+def assert_matches_oracle(oracle, sol, params, inputs, ref, keys, tables=None, **kw):
+    """Per-element checks of sol's last step against the FP32 oracle step
+    ``ref`` from ``inputs`` = (x, v, bx, psi, dt): 1e-4 for the terms before
+    the solve and for x (in units of the spacing), the FP32 noise rule against
+    an FP64 oracle step at the same iteration count for the Jacobi outputs."""
+    x, v, bx, psi, dt = inputs
+    fl = parity_floors(params, dt)
+    truth = None
+    for k in keys:
+        got = getattr(sol, _FIELDS[k]).numpy()
+        if k in _JACOBI:
+            if truth is None:
+                truth = _oracle_step(oracle, params, x, v, bx, psi, dt, 1.0 / dt, precision="f64", tables=tables,
+                                     **dict(kw, fixed_iters=int(ref["iterations"])))
+            assert_jacobi(got, ref[k], truth[k], fl[k], k)
+        else:
+            assert_elem(got, ref[k], fl[k], k, x_like=(k == "x"))
+
+
+def _at_reference_count(sol, params, scene, x, v, dt, ref, pressure=None):
+    """sol itself when its last step ran the reference's iteration count,
+    else a twin context stepped from the same inputs with that many fixed
+    iterations (the caller closes it if it is not sol)."""
+    if sol.last_stats["iterations"] == int(ref["iterations"]):
+        return sol
+    twin = _solver(params.replace(fixed_iters=int(ref["iterations"])), scene)
+    twin.set_state(x, v)
+    if pressure is not None:
+        twin.set_pressure(pressure)
+    twin.set_dt(dt, 1.0 / dt)
+    twin.step()
+    assert twin.last_stats["iterations"] == int(ref["iterations"])
+    return twin
 
 
 def test_dam_break_8k_vs_oracle(oracle):
@@ -139,32 +179,26 @@ def test_dam_break_8k_vs_oracle(oracle):
     op = oracle.reference_params(diameter=params.diameter, gravity=params.gravity, w_size=1024, g_size=1024)
     from warpsph_b200.tables import kernel_tables
 
-    assert normrel(psi, oracle.boundary_psi(op, scene.boundary_x, tables=kernel_tables(params))) < 1e-5
+    assert_elem(psi, oracle.boundary_psi(op, scene.boundary_x, tables=kernel_tables(params)), 0.0, "psi", bar=1e-5)
     for warm in (0, 30):
         if warm:
             sol.steps(warm)
         x, v = sol.x.numpy(), sol.v.numpy()
         dt = sol.dt
         ref = _oracle_step(oracle, params, x, v, scene.boundary_x, psi, dt, 1.0 / dt)
-        truth = _oracle_step(oracle, params, x, v, scene.boundary_x, psi, dt, 1.0 / dt, precision="f64")
         sol.set_state(x, v)
         sol.set_dt(dt, 1.0 / dt)
         sol.step()
         nb = sol.get_neighbors(with_boundary=True)
         assert csr_equal(nb["ff_off"], nb["ff_idx"], ref["ff_off"], ref["ff_idx"])
         assert csr_equal(nb["fb_off"], nb["fb_idx"], ref["fb_off"], ref["fb_idx"])
-        assert normrel(sol.rho.numpy(), ref["rho"]) < RTOL
-        assert normrel(sol.rho_adv.numpy(), ref["rho_adv"]) < RTOL
-        assert normrel(sol.term_a_ii.numpy(), ref["a_ii"]) < RTOL
+        inputs = (x, v, scene.boundary_x, psi, dt)
+        assert_matches_oracle(oracle, sol, params, inputs, ref, ("rho", "rho_adv", "d_ii", "a_ii"))
         assert abs(sol.last_stats["iterations"] - ref["iterations"]) <= 1
-        if sol.last_stats["iterations"] == ref["iterations"]:
-            assert normrel(sol.p.numpy(), ref["p"]) < RTOL
-            assert normrel(sol.v.numpy(), ref["v"]) < RTOL
-            assert normrel(sol.x.numpy(), ref["x"]) < 1e-6
-            # error against FP64 truth stays at the FP32 mirror's level
-            e_gpu = normrel(sol.rho.numpy(), truth["rho"])
-            e_f32 = normrel(ref["rho"], truth["rho"])
-            assert e_gpu < max(10 * e_f32, 1e-6)
+        src = _at_reference_count(sol, params, scene, x, v, dt, ref)
+        assert_matches_oracle(oracle, src, params, inputs, ref, ("p", "s", "v", "x"))
+        if src is not sol:
+            src.close()
     sol.close()
 
 
@@ -188,14 +222,13 @@ def test_viscous_dam_break_vs_oracle(oracle):
     sol.step()
     nb = sol.get_neighbors(with_boundary=True)
     assert csr_equal(nb["ff_off"], nb["ff_idx"], ref["ff_off"], ref["ff_idx"])
-    assert normrel(sol.rho.numpy(), ref["rho"]) < RTOL
-    assert normrel(sol.v_adv.numpy(), ref["v_adv"]) < RTOL
-    assert normrel(sol.rho_adv.numpy(), ref["rho_adv"]) < RTOL
-    assert normrel(sol.term_a_ii.numpy(), ref["a_ii"]) < RTOL
+    inputs = (x, v, scene.boundary_x, psi, dt)
+    assert_matches_oracle(oracle, sol, params, inputs, ref, ("rho", "v_adv", "rho_adv", "a_ii"))
     assert abs(sol.last_stats["iterations"] - ref["iterations"]) <= 1
-    if sol.last_stats["iterations"] == ref["iterations"]:
-        assert normrel(sol.p.numpy(), ref["p"]) < RTOL
-        assert normrel(sol.v.numpy(), ref["v"]) < RTOL
+    src = _at_reference_count(sol, params, scene, x, v, dt, ref)
+    assert_matches_oracle(oracle, src, params, inputs, ref, ("p", "v", "x"))
+    if src is not sol:
+        src.close()
     # the viscous term is really on: v_adv differs from v - g dt y
     base = v.copy()
     base[:, 1] -= params.gravity * dt
@@ -232,9 +265,8 @@ def test_table_gradient_path(oracle, g_size):
                                  g_size=g_size)
     ref = oracle.step(op, x, v, scene.boundary_x, None, psi, dt, 1.0 / dt, tables=(w, g), fixed_iters=6)
     assert sol.last_stats["iterations"] == 6
-    assert normrel(sol.p.numpy(), ref["p"]) < RTOL
-    assert normrel(sol.term_Ap_i.numpy(), ref["Ap"]) < RTOL
-    assert normrel(sol.v.numpy(), ref["v"]) < RTOL
+    assert_matches_oracle(oracle, sol, params, (x, v, scene.boundary_x, psi, dt), ref, ("a_ii", "p", "Ap", "v"),
+                          tables=(w, g))
     sol.close()
 
 
@@ -255,8 +287,8 @@ def test_warm_start_half_vs_oracle(oracle):
     sol2.set_pressure(p)
     sol2.set_dt(sol.dt, 1.0 / sol.dt)
     sol2.step()
-    assert normrel(sol2.p.numpy(), ref["p"]) < RTOL
-    assert normrel(sol2.v.numpy(), ref["v"]) < RTOL
+    assert_matches_oracle(oracle, sol2, params, (x, v, scene.boundary_x, psi, sol.dt), ref, ("p", "v", "x"),
+                          p=p, warm_start=1)
     sol.close()
     sol2.close()
 
@@ -285,9 +317,8 @@ def test_warm_continue_after_capped_solve_vs_oracle(oracle):
     assert sol.last_stats["iterations"] == max_loop + 1
     ref = _oracle_step(oracle, params, x, v, scene.boundary_x, psi, dt, 1.0 / dt, p=p, warm_start=2,
                        fixed_iters=max_loop)
-    assert normrel(sol.p.numpy(), ref["p"]) < RTOL
-    assert normrel(sol.v.numpy(), ref["v"]) < RTOL
-    assert normrel(sol.x.numpy(), ref["x"]) < RTOL
+    assert_matches_oracle(oracle, sol, params, (x, v, scene.boundary_x, psi, dt), ref, ("p", "v", "x"),
+                          p=p, warm_start=2)
     # without warm_continue the second step starts from the network's prediction
     plain = _solver(params.replace(warm_continue=False), scene)
     plain.steps(2)
@@ -358,9 +389,10 @@ def test_empty_fluid_and_isolated_particle(oracle):
     sol.step()
     psi = sol.boundary_phi.numpy()
     ref = _oracle_step(oracle, params, x, np.zeros_like(x), bx, psi, params.dt_max, 1 / params.dt_max)
-    assert normrel(sol.p.numpy(), ref["p"]) < RTOL
     assert ref["p"][0] > 1e8
-    assert normrel(sol.v.numpy(), ref["v"]) < RTOL
+    assert sol.last_stats["iterations"] == ref["iterations"]
+    assert_matches_oracle(oracle, sol, params, (x, np.zeros_like(x), bx, psi, params.dt_max), ref,
+                          ("rho", "a_ii", "p", "v", "x"))
     sol.close()
 
 
@@ -420,11 +452,13 @@ def test_no_boundary_free_fall_vs_oracle(oracle):
     sol.step()
     nb = sol.get_neighbors()
     assert csr_equal(nb["ff_off"], nb["ff_idx"], ref["ff_off"], ref["ff_idx"])
-    assert normrel(sol.rho.numpy(), ref["rho"]) < RTOL
+    inputs = (x, np.zeros_like(x), np.zeros((0, 3), np.float32), np.zeros(0, np.float32), params.dt_max)
+    assert_matches_oracle(oracle, sol, params, inputs, ref, ("rho", "rho_adv", "a_ii"))
     assert abs(sol.last_stats["iterations"] - ref["iterations"]) <= 1
-    if sol.last_stats["iterations"] == ref["iterations"]:
-        assert normrel(sol.p.numpy(), ref["p"]) < RTOL
-        assert normrel(sol.v.numpy(), ref["v"]) < RTOL
+    src = _at_reference_count(sol, params, sc, x, np.zeros_like(x), params.dt_max, ref)
+    assert_matches_oracle(oracle, src, params, inputs, ref, ("p", "v", "x"))
+    if src is not sol:
+        src.close()
     sol.close()
 
 
@@ -452,7 +486,7 @@ def test_coincident_particles_vs_oracle(oracle):
     sol.step()
     nb = sol.get_neighbors()
     assert csr_equal(nb["ff_off"], nb["ff_idx"], ref["ff_off"], ref["ff_idx"])
-    assert normrel(sol.rho.numpy(), ref["rho"]) < RTOL  # density has no r^2 division
+    assert_elem(sol.rho.numpy(), ref["rho"], parity_floors(params, params.dt_max)["rho"], "rho")  # no r^2 division
     dup = np.arange(0, len(block.fluid_x), 37)
     assert np.isnan(ref["v_adv"][dup]).all()             # the reference's 0 * inf
     v_adv = sol.v_adv.numpy()
