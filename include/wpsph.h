@@ -87,6 +87,10 @@ typedef struct SphParams {
                             cap, the next step of that scene starts from the capped solve's final
                             pressure (or from sph_set_pressure's, if called in between) instead
                             of the network's prediction; sph_set_fluid forgets the cap */
+  int32_t jacobi_plain_loads; /* 1: the solve's second pass gathers neighbour positions with plain
+                            global loads; 0 (default): through the texture path (a texture object
+                            over the same array), which the first pass's gathers do not use, so the
+                            two kinds of gather share the load; same values, same results */
 } SphParams;
 
 typedef struct SphStepStats { /* for a batch: max over scenes, dt and time of scene 0 */

@@ -356,6 +356,25 @@ def test_deterministic_and_graph_equivalent():
         assert np.array_equal(a, b)
 
 
+def test_texture_gathers_equal_plain_loads():
+    """The solve's second pass reads neighbour positions through the texture
+    path by default; the values are the same words, so every step is the
+    same as with plain loads, bit for bit (learned start, continuation)."""
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+
+    scene = preset_scene("dam_break_8k")
+    outs = []
+    for plain in (False, True):
+        sol = _solver(preset_params("dam_break_8k", warm_start="mlp", warm_continue=True, jacobi_plain_loads=plain),
+                      scene)
+        sol.steps(25)
+        outs.append((sol.x.numpy(), sol.v.numpy(), sol.p.numpy(), sol.last_stats["iterations"]))
+        sol.close()
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a, b)
+
+
 def test_capacity_auto_grow():
     from warpsph_b200.params import preset_params
     from warpsph_b200.scenes import preset_scene

@@ -866,10 +866,7 @@ int sph_create(const SphParams* params, SphCtx** out) {
   ctx->jac_unroll = P.jacobi_unroll ? P.jacobi_unroll : 4;
   if (!sph::jacobi_variant_ok(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll)) return bail(SPH_E_INVALID);
   ctx->chunk = ctx->jac_block * ctx->jac_ppt;
-  {
-    const char* e = std::getenv("WPSPH_JACOBI_TEX");
-    ctx->jac_tex = e && e[0] == '1';
-  }
+  ctx->jac_tex = (P.jacobi_plain_loads == 0);
   if (sph::jacobi_config(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll, ctx->c.sg, ctx->g_spline, &ctx->blocks_per_sm,
                          &ctx->jac_smem, ctx->jac_tex) != cudaSuccess ||
       ctx->blocks_per_sm < 1)
