@@ -87,10 +87,11 @@ typedef struct SphParams {
                             cap, the next step of that scene starts from the capped solve's final
                             pressure (or from sph_set_pressure's, if called in between) instead
                             of the network's prediction; sph_set_fluid forgets the cap */
-  int32_t jacobi_plain_loads; /* 1: the solve's second pass gathers neighbour positions with plain
-                            global loads; 0 (default): through the texture path (a texture object
-                            over the same array), which the first pass's gathers do not use, so the
-                            two kinds of gather share the load; same values, same results */
+  int32_t plain_loads;    /* 1: every neighbour gather uses plain global loads; 0 (default): the
+                            gathers of arrays that a kernel only reads (the solve's second-pass
+                            positions, the neighbour build's positions and velocities) go through
+                            the texture path, from texture objects over the same arrays, beside
+                            the plain loads of the rest; same values, same results */
 } SphParams;
 
 typedef struct SphStepStats { /* for a batch: max over scenes, dt and time of scene 0 */

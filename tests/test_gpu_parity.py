@@ -357,7 +357,8 @@ def test_deterministic_and_graph_equivalent():
 
 
 def test_texture_gathers_equal_plain_loads():
-    """The solve's second pass reads neighbour positions through the texture
+    """The solve's second pass (neighbour positions) and the neighbour
+    build's second phase (positions, velocities) read through the texture
     path by default; the values are the same words, so every step is the
     same as with plain loads, bit for bit (learned start, continuation)."""
     from warpsph_b200.params import preset_params
@@ -366,7 +367,7 @@ def test_texture_gathers_equal_plain_loads():
     scene = preset_scene("dam_break_8k")
     outs = []
     for plain in (False, True):
-        sol = _solver(preset_params("dam_break_8k", warm_start="mlp", warm_continue=True, jacobi_plain_loads=plain),
+        sol = _solver(preset_params("dam_break_8k", warm_start="mlp", warm_continue=True, plain_loads=plain),
                       scene)
         sol.steps(25)
         outs.append((sol.x.numpy(), sol.v.numpy(), sol.p.numpy(), sol.last_stats["iterations"]))

@@ -59,7 +59,7 @@ class SphParams(ctypes.Structure):
         ("use_graph", ctypes.c_int32), ("device", ctypes.c_int32), ("block_size", ctypes.c_int32),
         ("timeout_ms", ctypes.c_int32), ("jacobi_block", ctypes.c_int32), ("jacobi_ppt", ctypes.c_int32),
         ("jacobi_unroll", ctypes.c_int32), ("move_boundary", ctypes.c_int32),
-        ("warm_continue", ctypes.c_int32), ("jacobi_plain_loads", ctypes.c_int32),
+        ("warm_continue", ctypes.c_int32), ("plain_loads", ctypes.c_int32),
     ]
 
 

@@ -36,9 +36,15 @@ namespace sph {
 // rows of 5 x-adjacent half cells with the exact float32 test and write the hits
 // into the particle's ELL list.  Only a compare and a predicated store run per
 // candidate, so the warp stays converged; loads are issued four at a time.
+// A record of a read-only float4 array, through the texture path when the
+// array has a texture object (tex != 0), else with a read-only global load.
+__device__ __forceinline__ float4 ro_load(const float4* __restrict__ p, unsigned long long tex, int j) {
+  return tex ? tex1Dfetch<float4>(cudaTextureObject_t(tex), j) : __ldg(p + j);
+}
+
 __device__ inline int filter_rows(const Grid& g, int base, int3 ci, const int* __restrict__ cell_start,
                                   const float4* __restrict__ pts, float4 xi, float r2_limit, int self, int* out,
-                                  int K) {
+                                  int K, unsigned long long tex = 0) {
   int cnt = 0;
   const int x0 = max(ci.x - kXReach, 0), x1 = min(ci.x + kXReach, g.nx - 1);
   for (int cz = max(ci.z - 1, 0); cz <= min(ci.z + 1, g.nz - 1); ++cz) {
@@ -49,7 +55,7 @@ __device__ inline int filter_rows(const Grid& g, int base, int3 ci, const int* _
       for (; j + 4 <= je; j += 4) {
         float4 q[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) q[u] = __ldg(pts + j + u);
+        for (int u = 0; u < 4; ++u) q[u] = ro_load(pts, tex, j + u);
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const float r2 = dist2_rn(xi.x, xi.y, xi.z, q[u].x, q[u].y, q[u].z);
@@ -60,7 +66,7 @@ __device__ inline int filter_rows(const Grid& g, int base, int3 ci, const int* _
         }
       }
       for (; j < je; ++j) {
-        const float4 q = __ldg(pts + j);
+        const float4 q = ro_load(pts, tex, j);
         const float r2 = dist2_rn(xi.x, xi.y, xi.z, q.x, q.y, q.z);
         if (r2 < r2_limit && j != self) {
           if (cnt < K) out[(long long)cnt * kWarp] = j;
@@ -143,7 +149,7 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Ker& ker) {
 
     // phase 1: neighbour lists (the advect pass reads the lists built before)
     if (kLists) {
-      cnt = filter_rows(g, fr.base, ci, a.cell_start, a.pos, xi, c.r2_limit, i, nbr, K);
+      cnt = filter_rows(g, fr.base, ci, a.cell_start, a.pos, xi, c.r2_limit, i, nbr, K, a.cand_tex);
       if (a.nb > 0) cntb = filter_rows(g, fr.base, ci, a.bcell_start, a.bpos, xi, c.r2_limit, -1, nbrb, KB);
     } else {
       cnt = a.cnt_ff[i];
@@ -165,6 +171,9 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Ker& ker) {
       div += (vax - vj.x) * gx + (vay - (vj.y + gdt)) * gy + (vaz - vj.z) * gz;
     };
     const int nf = min(cnt, K);
+    // the neighbours' velocities through the texture path only when they
+    // are the step's velocities (not the v_adv the viscosity pass wrote)
+    const unsigned long long vtex = (MODE == kBuildAdvect) ? 0ull : a.vel_tex;
     int k = 0;
     for (; k + 4 <= nf; k += 4) {
       int j[4];
@@ -173,15 +182,15 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Ker& ker) {
       for (int u = 0; u < 4; ++u) j[u] = nbr[(k + u) * kWarp];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        xj[u] = __ldg(a.pos + j[u]);
-        vj[u] = __ldg(vsrc + j[u]);
+        xj[u] = ro_load(a.pos, a.pos_tex, j[u]);
+        vj[u] = ro_load(vsrc, vtex, j[u]);
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) fluid(xj[u], vj[u]);
     }
     for (; k < nf; ++k) {
       const int j = nbr[k * kWarp];
-      fluid(__ldg(a.pos + j), __ldg(vsrc + j));
+      fluid(ro_load(a.pos, a.pos_tex, j), ro_load(vsrc, vtex, j));
     }
 
     float sWb = 0.f, Bx = 0.f, By = 0.f, Bz = 0.f, divb = 0.f;

@@ -86,6 +86,7 @@ struct SphCtx {
   int jac_block = 256, jac_ppt = 1, jac_unroll = 4;  // autotuner knobs of the solve
   bool jac_tex = false;                               // pass B reads x_j through the texture path
   cudaTextureObject_t pos_tex = 0;                    // over pos_w, when jac_tex
+  cudaTextureObject_t vel_tex = 0;                    // over vel_w, when jac_tex
   int stall_block = -1;                               // sph_test_stall_barrier
   int withhold_mma = 0;                               // sph_test_withhold_mma
   int chunk = 256;                                    // particles per solve chunk
@@ -455,21 +456,29 @@ int alloc_neighbors(SphCtx* ctx) {
   return SPH_OK;
 }
 
-// A 1-D texture object over the solve's position array (float4 per slot).
-int make_pos_texture(SphCtx* ctx) {
-  if (ctx->pos_tex) {
-    cudaDestroyTextureObject(ctx->pos_tex);
-    ctx->pos_tex = 0;
-  }
+// Whether the build's first phase reads its fluid candidates through the
+// texture path as well as the second phase's neighbour gathers.
+constexpr bool kBuildTexCandidates = false;
+
+// 1-D texture objects over the work arrays of positions and velocities
+// (float4 per slot): read-only gathers that then use the texture path.
+int make_textures(SphCtx* ctx) {
+  for (cudaTextureObject_t* t : {&ctx->pos_tex, &ctx->vel_tex})
+    if (*t) {
+      cudaDestroyTextureObject(*t);
+      *t = 0;
+    }
   if (!ctx->jac_tex) return SPH_OK;
-  cudaResourceDesc rd{};
-  rd.resType = cudaResourceTypeLinear;
-  rd.res.linear.devPtr = ctx->pos_w;
-  rd.res.linear.desc = cudaCreateChannelDesc<float4>();
-  rd.res.linear.sizeInBytes = sizeof(float4) * size_t(ctx->n_cap);
-  cudaTextureDesc td{};
-  td.readMode = cudaReadModeElementType;
-  CK(cudaCreateTextureObject(&ctx->pos_tex, &rd, &td, nullptr));
+  for (int k = 0; k < 2; ++k) {
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypeLinear;
+    rd.res.linear.devPtr = k == 0 ? static_cast<void*>(ctx->pos_w) : static_cast<void*>(ctx->vel_w);
+    rd.res.linear.desc = cudaCreateChannelDesc<float4>();
+    rd.res.linear.sizeInBytes = sizeof(float4) * size_t(ctx->n_cap);
+    cudaTextureDesc td{};
+    td.readMode = cudaReadModeElementType;
+    CK(cudaCreateTextureObject(k == 0 ? &ctx->pos_tex : &ctx->vel_tex, &rd, &td, nullptr));
+  }
   return SPH_OK;
 }
 
@@ -480,11 +489,11 @@ int alloc_fluid(SphCtx* ctx, int64_t n) {
   CK(dalloc(ctx->pos_s, m));
   CK(dalloc(ctx->vel_s, m));
   CK(dalloc(ctx->pos_w, m));
+  CK(dalloc(ctx->vel_w, m));
   {
-    const int rc = make_pos_texture(ctx);
+    const int rc = make_textures(ctx);
     if (rc) return rc;
   }
-  CK(dalloc(ctx->vel_w, m));
   CK(dalloc(ctx->orig_s, m));
   CK(dalloc(ctx->orig_w, m));
   CK(dalloc(ctx->p_s, m));
@@ -568,6 +577,9 @@ sph::BuildArgs build_args(SphCtx* ctx) {
   b.pos_q = ctx->pos_w;
   b.feat = (ctx->record_feat || ctx->P.warm_start == SPH_WARM_MLP) ? ctx->feat : nullptr;
   b.coltop = ctx->coltop;
+  b.pos_tex = ctx->jac_tex ? (unsigned long long)ctx->pos_tex : 0ull;
+  b.vel_tex = ctx->jac_tex ? (unsigned long long)ctx->vel_tex : 0ull;
+  b.cand_tex = kBuildTexCandidates ? b.pos_tex : 0ull;
   return b;
 }
 
@@ -866,7 +878,7 @@ int sph_create(const SphParams* params, SphCtx** out) {
   ctx->jac_unroll = P.jacobi_unroll ? P.jacobi_unroll : 4;
   if (!sph::jacobi_variant_ok(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll)) return bail(SPH_E_INVALID);
   ctx->chunk = ctx->jac_block * ctx->jac_ppt;
-  ctx->jac_tex = (P.jacobi_plain_loads == 0);
+  ctx->jac_tex = (P.plain_loads == 0);
   if (sph::jacobi_config(ctx->jac_block, ctx->jac_ppt, ctx->jac_unroll, ctx->c.sg, ctx->g_spline, &ctx->blocks_per_sm,
                          &ctx->jac_smem, ctx->jac_tex) != cudaSuccess ||
       ctx->blocks_per_sm < 1)
@@ -882,6 +894,7 @@ void sph_destroy(SphCtx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   if (ctx->pos_tex) cudaDestroyTextureObject(ctx->pos_tex);
+  if (ctx->vel_tex) cudaDestroyTextureObject(ctx->vel_tex);
   void* ptrs[] = {ctx->d_w, ctx->d_g, ctx->bpos, ctx->bvel, ctx->borig, ctx->bpos_t, ctx->bvel_t, ctx->borig_t,
                   ctx->bkey, ctx->brank, ctx->bsrc, ctx->bcell_start, ctx->pos_s, ctx->vel_s,
                   ctx->pos_w, ctx->vel_w, ctx->orig_s, ctx->orig_w, ctx->p_s, ctx->pprev_w, ctx->key, ctx->rank,

@@ -393,6 +393,9 @@ struct BuildArgs {
   float4* pos_q;           // the array `pos` points to: p0 / rho^2 goes into .w
   float* feat;             // optional MLP feature rows (n x kFeatures), NULL to skip
   const unsigned int* coltop;  // with feat: per grid column (x, z), the highest fluid y (ordered key)
+  // texture objects over pos and vel (0: plain read-only loads): the second
+  // phase's neighbour gathers, and (cand_tex) the first phase's candidates
+  unsigned long long pos_tex, vel_tex, cand_tex;
 };
 
 // Order-preserving uint key of a float (atomicMax on keys = max on floats);

@@ -45,7 +45,7 @@ class SolverParams:
     jacobi_unroll: int = 0        # solve neighbour-loop unroll (0 = 4)
     move_boundary: bool = False   # boundary moves with its velocities (DYNAMIC_SCENE, main.py:20)
     warm_continue: bool = False   # "mlp": a step after a capped solve starts from that solve's pressure
-    jacobi_plain_loads: bool = False  # solve's second pass: plain loads instead of the texture path
+    plain_loads: bool = False     # neighbour gathers: plain loads instead of the texture path
     dt0: float | None = None      # None: TIME_STEP_MAX (IISPH.py:747)
     domain_min: tuple = (0.0, 0.0, 0.0)
     domain_max: tuple = (0.0, 0.0, 0.0)
@@ -115,7 +115,7 @@ class SolverParams:
         p.jacobi_unroll = self.jacobi_unroll
         p.move_boundary = int(self.move_boundary)
         p.warm_continue = int(self.warm_continue)
-        p.jacobi_plain_loads = int(self.jacobi_plain_loads)
+        p.plain_loads = int(self.plain_loads)
         return p
 
     @classmethod
