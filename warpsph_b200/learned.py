@@ -114,12 +114,15 @@ def evaluate(blob, feat, target=None, device=0):
     return pred, float(grad[-1]), grad[:-1]
 
 
-def collect(scenes, steps, per_step, params_for, seed=0, warm="zero", skip=0, skip_capped=True):
+def collect(scenes, steps, per_step, params_for, seed=0, warm="zero", skip=0, skip_capped=True,
+            early_steps=0, early_boost=1):
     """Run each scene for ``steps`` steps, sampling ``per_step`` (input, target)
-    pairs per step after the first ``skip`` steps.  With ``skip_capped``,
-    steps whose solve stopped at the iteration cap are left out: their
-    pressure is not a solution of the step's system.  ``params_for(scene)``
-    gives the SolverParams."""
+    pairs per step after the first ``skip`` steps, ``early_boost`` times as
+    many in the first ``early_steps`` (the start-up transient, a small share
+    of the steps but where a start saves the most iterations).  With
+    ``skip_capped``, steps whose solve stopped at the iteration cap are left
+    out: their pressure is not a solution of the step's system.
+    ``params_for(scene)`` gives the SolverParams."""
     from .solver import IISPH
 
     rng = np.random.default_rng(seed)
@@ -135,7 +138,8 @@ def collect(scenes, steps, per_step, params_for, seed=0, warm="zero", skip=0, sk
             if k < skip or (skip_capped and sol.last_stats["flags"] & _lib.SPH_F_NOT_CONVERGED):
                 continue
             _lib.check(sol._ctx, sol._lib.sph_get_features(sol._ctx, _lib.ptr(f), _lib.ptr(t)))
-            pick = rng.choice(n, size=min(per_step, n), replace=False)
+            want = per_step * (early_boost if k < early_steps else 1)
+            pick = rng.choice(n, size=min(want, n), replace=False)
             feats.append(f[pick].copy())
             targets.append(t[pick].copy())
         sol.close()

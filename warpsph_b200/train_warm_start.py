@@ -43,13 +43,16 @@ def main():
     ap.add_argument("--skip", type=int, default=0, help="start-up steps of each scene left out of the data")
     ap.add_argument("--rounds", type=int, default=2, help="on-policy rounds after the first fit")
     ap.add_argument("--alpha", type=float, default=1.0, help="resampling weight 1 + alpha * max(target, 0)")
+    ap.add_argument("--early-steps", type=int, default=0, help="steps of each scene sampled early-boost times as densely")
+    ap.add_argument("--early-boost", type=int, default=1)
     a = ap.parse_args()
     scenes = batched_scenes(count=a.scenes)
     per_step = max(1, a.pairs // (a.scenes * max(1, a.steps - a.skip)))
     t0 = time.time()
     params = SolverParams(diameter=0.01, gravity=9.81, w_table_size=1024, g_table_size=1024)
+    early = dict(early_steps=a.early_steps, early_boost=a.early_boost)
     feat, target = learned.collect(scenes, a.steps, per_step, lambda sc: params, seed=a.seed, warm="zero",
-                                   skip=a.skip)
+                                   skip=a.skip, **early)
     t_collect = time.time() - t0
     t1 = time.time()
     blob, losses = learned.train(feat, target, epochs=a.epochs, lr=a.lr, seed=a.seed)
@@ -58,13 +61,14 @@ def main():
         t0 = time.time()
         policy = params.replace(extra={"mlp_blob": blob})
         feat, target = learned.collect(scenes, a.steps, per_step, lambda sc: policy, seed=a.seed + r, warm="mlp",
-                                       skip=a.skip)
+                                       skip=a.skip, **early)
         feat, target = learned.weighted_resample(feat, target, a.alpha, seed=a.seed + r)
         t_collect += time.time() - t0
         t1 = time.time()
         blob, losses = learned.train(feat, target, epochs=a.epochs, lr=a.lr, seed=a.seed)
         t_train += time.time() - t1
-    meta = dict(pairs=len(target), scenes=a.scenes, steps=a.steps, skip=a.skip, epochs=a.epochs, lr=a.lr,
+    meta = dict(pairs=len(target), scenes=a.scenes, steps=a.steps, skip=a.skip, early_steps=a.early_steps,
+                early_boost=a.early_boost, epochs=a.epochs, lr=a.lr,
                 rounds=a.rounds, alpha=a.alpha, losses=losses.tolist(), collect_s=t_collect, train_s=t_train)
     learned.save(a.out, blob, meta=json.dumps(meta))
     print(json.dumps(meta))
