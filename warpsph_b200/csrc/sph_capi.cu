@@ -65,6 +65,8 @@ struct SphCtx {
   float *p_s = nullptr, *pprev_w = nullptr;
   int *key = nullptr, *rank = nullptr, *sort_src = nullptr, *sort_orig = nullptr;
   int *cell_count = nullptr, *cell_start = nullptr, *scan_part = nullptr;
+  unsigned long long* scan_status = nullptr;  // single-pass scan: tile states, then the ticket
+  int scan_tiles_cap = 0;
   unsigned int* coltop = nullptr;  // per grid column, the highest fluid y (warm-start input 10)
   int *nbr_ff = nullptr, *cnt_ff = nullptr, *nbr_fb = nullptr, *cnt_fb = nullptr;
   float* rho = nullptr;
@@ -333,6 +335,8 @@ int set_grid(SphCtx* ctx, const float* xf, int64_t n) {
     CK(dalloc(ctx->cell_start, ctx->total_cells + 1));
     CK(dalloc(ctx->bcell_start, ctx->total_cells + 1));
     CK(dalloc(ctx->scan_part, ctx->total_cells / 4096 + 2));
+    ctx->scan_tiles_cap = ctx->total_cells / 4096 + 2;
+    CK(dalloc(ctx->scan_status, size_t(ctx->scan_tiles_cap) + 1));
     CK(dalloc(ctx->coltop, ctx->total_cells));
     ctx->ncells_cap = ctx->total_cells;
   }
@@ -540,6 +544,9 @@ sph::SortArgs fluid_sort_args(SphCtx* ctx) {
   s.cell_count = ctx->cell_count;
   s.cell_start = ctx->cell_start;
   s.scan_part = ctx->scan_part;
+  s.scan_status = ctx->scan_status;
+  s.scan_ticket = reinterpret_cast<unsigned int*>(ctx->scan_status + ctx->scan_tiles_cap);
+  s.err = &ctx->acc->flags;
   s.sort_src = ctx->sort_src;
   s.sort_orig = ctx->sort_orig;
   return s;
@@ -898,7 +905,7 @@ void sph_destroy(SphCtx* ctx) {
   void* ptrs[] = {ctx->d_w, ctx->d_g, ctx->bpos, ctx->bvel, ctx->borig, ctx->bpos_t, ctx->bvel_t, ctx->borig_t,
                   ctx->bkey, ctx->brank, ctx->bsrc, ctx->bcell_start, ctx->pos_s, ctx->vel_s,
                   ctx->pos_w, ctx->vel_w, ctx->orig_s, ctx->orig_w, ctx->p_s, ctx->pprev_w, ctx->key, ctx->rank,
-                  ctx->sort_src, ctx->sort_orig, ctx->cell_count, ctx->cell_start, ctx->scan_part, ctx->coltop, ctx->nbr_ff,
+                  ctx->sort_src, ctx->sort_orig, ctx->cell_count, ctx->cell_start, ctx->scan_part, ctx->scan_status, ctx->coltop, ctx->nbr_ff,
                   ctx->cnt_ff, ctx->nbr_fb, ctx->cnt_fb, ctx->rho, ctx->bvec, ctx->dii_aii, ctx->vadv, ctx->a4,
                   ctx->p_a, ctx->p_b, ctx->Ap, ctx->pmlp, ctx->feat, ctx->p_start, ctx->mlp, ctx->stage, ctx->partials, ctx->st, ctx->acc, ctx->ring,
                   ctx->d_scenes, ctx->d_chunks, ctx->d_chunk_scene,

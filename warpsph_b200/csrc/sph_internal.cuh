@@ -358,7 +358,13 @@ struct SortArgs {
   int* rank;
   int* cell_count;     // ncells, zeroed
   int* cell_start;     // ncells + 1
-  int* scan_part;      // partial sums per scan block
+  int* scan_part;      // partial sums per scan block (two-kernel scan)
+  // single-pass scan (used when scan_status != nullptr): per tile of cells a
+  // 64-bit status word (flag << 32 | sum), zeroed by k_cell_keys, the tile
+  // ticket, and where a look-back that waited too long sets SPH_F_TIMEOUT
+  unsigned long long* scan_status;
+  unsigned int* scan_ticket;
+  int* err;
   int* sort_src;       // new index -> old index
   int* sort_orig;      // new index -> original id
 };

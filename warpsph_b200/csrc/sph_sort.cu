@@ -11,11 +11,14 @@
 //
 //   1. k_cell_keys   cell key per particle; rank inside its cell from a
 //                    warp-aggregated atomic on the cell counter
-//   2. k_scan_part   per-block sums of the cell counters
-//   3. k_scan_final  exclusive scan -> cell_start (each block first sums the
-//                    partials before it: no inter-block waiting)
-//   4. k_scatter     new slot = cell_start[key] + rank
-//   5. k_cell_sort   order each cell's slots by original id
+//   2. k_scan_onepass  exclusive scan -> cell_start in one kernel: each tile
+//                    of cells publishes its sum, then looks back over the
+//                    tiles before it (decoupled look-back) for its prefix
+//      (or, where no status buffer is given, k_scan_part: per-block sums of
+//      the cell counters, then k_scan_final: each block first sums the
+//      partials before it, no inter-block waiting)
+//   3. k_scatter     new slot = cell_start[key] + rank
+//   4. k_cell_sort   order each cell's slots by original id
 #include "sph_internal.cuh"
 
 namespace sph {
@@ -23,9 +26,15 @@ namespace sph {
 constexpr int kScanThreads = 512;
 constexpr int kScanItems = 8;  // cells per thread
 constexpr int kScanTile = kScanThreads * kScanItems;
+int scan_tiles(int ncells) { return (ncells + kScanTile - 1) / kScanTile; }
 
-__global__ void k_cell_keys(SortArgs a) {
+__global__ void k_cell_keys(SortArgs a, int scan_tiles) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a.scan_status && blockIdx.x == 0) {
+    // the single-pass scan's tile states and ticket start from zero
+    for (int t = threadIdx.x; t < scan_tiles; t += blockDim.x) a.scan_status[t] = 0ull;
+    if (threadIdx.x == 0) *a.scan_ticket = 0u;
+  }
   bool live = i < a.n;
   int key = -1;
   if (live) {
@@ -124,6 +133,100 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const int* __restri
   if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) start[ncells] = n;
 }
 
+// Tile states of the single-pass scan: flag in the high word.
+constexpr unsigned long long kTileAggregate = 1ull << 32;  // the tile's own sum is published
+constexpr unsigned long long kTilePrefix = 2ull << 32;     // the inclusive prefix through the tile
+constexpr long long kLookBackPolls = 1ll << 22;            // bound on one look-back wait
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Exclusive scan of the cell counters into cell_start in one kernel.  Tiles
+// are taken in ticket order, so every tile before this one has started and
+// publishes its sum without waiting on anything: each look-back wait ends.
+// It is still bounded (kLookBackPolls); if one ran out, SPH_F_TIMEOUT is set
+// and the step's results are discarded by the host.
+__global__ void __launch_bounds__(kScanThreads) k_scan_onepass(const int* __restrict__ count, int ncells,
+                                                               unsigned long long* status, unsigned int* ticket,
+                                                               int* start, int n, int* err) {
+  __shared__ int s_tile, s_pre;
+  __shared__ int warp_tot[kScanThreads / 32];
+  if (threadIdx.x == 0) s_tile = int(atomicAdd(ticket, 1u));
+  __syncthreads();
+  const int tile = s_tile;
+  const int base = tile * kScanTile + threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int tot = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int c = base + k;
+    v[k] = (c < ncells) ? count[c] : 0;
+    tot += v[k];
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int inc = tot;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) warp_tot[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    const int t = (lane < kScanThreads / 32) ? warp_tot[lane] : 0;
+    int ti = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, ti, o);
+      if (lane >= o) ti += u;
+    }
+    if (lane < kScanThreads / 32) warp_tot[lane] = ti - t;
+    if (lane == kScanThreads / 32 - 1) {
+      // ti is the tile's sum: publish it, find the prefix, publish that
+      const unsigned int agg = unsigned(ti);
+      int pre = 0;
+      if (tile == 0) {
+        st_release_u64(status, kTilePrefix | agg);
+      } else {
+        st_release_u64(status + tile, kTileAggregate | agg);
+        long long polls = 0;
+        for (int t = tile - 1; t >= 0;) {
+          const unsigned long long st = ld_acquire_u64(status + t);
+          const unsigned long long flag = st & ~0xffffffffull;
+          if (flag == 0ull) {
+            if (++polls > kLookBackPolls) {
+              atomicOr(err, SPH_F_TIMEOUT);
+              break;
+            }
+            __nanosleep(32);
+            continue;
+          }
+          pre += int(unsigned(st & 0xffffffffull));
+          if (flag == kTilePrefix) break;
+          --t;
+        }
+        st_release_u64(status + tile, kTilePrefix | unsigned(pre + int(agg)));
+      }
+      s_pre = pre;
+    }
+  }
+  __syncthreads();
+  int run = s_pre + warp_tot[w] + inc - tot;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int c = base + k;
+    if (c < ncells) start[c] = run;
+    run += v[k];
+  }
+  if (tile == int(gridDim.x) - 1 && threadIdx.x == 0) start[ncells] = n;
+}
+
 __global__ void k_scatter(SortArgs a) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
@@ -191,10 +294,15 @@ cudaError_t launch_sort(const SortArgs& a, int ncells, cudaStream_t s) {
   if (e != cudaSuccess) return e;
   const int T = 256;
   int gb = (a.n + T - 1) / T;
-  k_cell_keys<<<gb, T, 0, s>>>(a);
   int tiles = (ncells + kScanTile - 1) / kScanTile;
-  k_scan_part<<<tiles, kScanThreads, 0, s>>>(a.cell_count, ncells, a.scan_part);
-  k_scan_final<<<tiles, kScanThreads, 0, s>>>(a.cell_count, ncells, a.scan_part, a.cell_start, a.n);
+  k_cell_keys<<<gb, T, 0, s>>>(a, tiles);
+  if (a.scan_status) {
+    k_scan_onepass<<<tiles, kScanThreads, 0, s>>>(a.cell_count, ncells, a.scan_status, a.scan_ticket, a.cell_start,
+                                                 a.n, a.err);
+  } else {
+    k_scan_part<<<tiles, kScanThreads, 0, s>>>(a.cell_count, ncells, a.scan_part);
+    k_scan_final<<<tiles, kScanThreads, 0, s>>>(a.cell_count, ncells, a.scan_part, a.cell_start, a.n);
+  }
   k_scatter<<<gb, T, 0, s>>>(a);
   k_cell_sort<<<(ncells + T - 1) / T, T, 0, s>>>(a.cell_start, ncells, a.sort_src, a.sort_orig);
   return cudaGetLastError();
