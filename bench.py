@@ -35,9 +35,9 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "IISPH steps/s at 1M particles, 0.1% density err; learned warm-start vs plain"
 PRESET = "dam_break_1m"
-# cell_keys, scan_part, scan_final, scatter, cell_sort, gather, build, jacobi
+# cell_keys, scan_onepass, scatter, cell_sort, gather, build, jacobi
 # (+ column_top and mlp_infer with the learned warm start)
-KERNELS_PER_STEP = 8
+KERNELS_PER_STEP = 7
 
 
 def kernels_per_step(warm: str) -> int:
