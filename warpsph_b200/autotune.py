@@ -2,14 +2,17 @@
 
 Knobs: threads per block of the neighbour build (`block_size`), and of the
 persistent pressure solve (`jacobi_block`), particles per solve thread
-(`jacobi_ppt`, so one solve chunk holds jacobi_block * jacobi_ppt particles)
-and the unroll of the solve's neighbour loops (`jacobi_unroll`).  None of
-them changes the arithmetic, only how work maps onto the SMs.
+(`jacobi_ppt`, so one solve chunk holds jacobi_block * jacobi_ppt particles),
+the unroll of the solve's neighbour loops (`jacobi_unroll`), and whether the
+read-only neighbour gathers use the texture path or plain loads
+(`plain_loads`).  None of them changes the arithmetic, only how work maps
+onto the SMs and which load path carries it.
 
 Each candidate runs the caller's own scene (or batch of scenes) on a fresh
 solver: `warm` untimed steps, then `steps` steps timed with CUDA events.  The
 build knob is tuned first with the solve at its default, then the solve knobs
-jointly.  Results are cached in JSON keyed by GPU name and workload size.
+jointly, then the load path at the best shape.  Results are cached in JSON
+keyed by GPU name and workload size.
 """
 
 from __future__ import annotations
@@ -26,7 +29,7 @@ CACHE = Path(os.environ.get("WPSPH_AUTOTUNE_CACHE", Path.home() / ".cache" / "wa
 def _signature(scenes, params) -> str:
     n = sum(s.n for s in scenes)
     nb = sum(s.boundary_n for s in scenes)
-    return f"scenes={len(scenes)},n={n},nb={nb},d={params.diameter},warm={params.warm_start}"
+    return f"scenes={len(scenes)},n={n},nb={nb},d={params.diameter},warm={params.warm_start},v2"
 
 
 def _time(scenes, params, warm, steps) -> float:
@@ -53,7 +56,7 @@ def _time(scenes, params, warm, steps) -> float:
 
 def autotune(scenes, params, warm=10, steps=20, use_cache=True, verbose=False) -> dict:
     """Best knob values for this workload: {'block_size', 'jacobi_block',
-    'jacobi_ppt', 'jacobi_unroll', 'ms_per_step', 'trials'}."""
+    'jacobi_ppt', 'jacobi_unroll', 'plain_loads', 'ms_per_step', 'trials'}."""
     import torch
 
     key = f"{torch.cuda.get_device_name(params.device)}|{_signature(scenes, params)}"
@@ -80,8 +83,15 @@ def autotune(scenes, params, warm=10, steps=20, use_cache=True, verbose=False) -
             print("solve", blk, ppt, unr, t)
         if t < best_t:
             best, best_t = (blk, ppt, unr), t
-    res = {"block_size": best_build, "jacobi_block": best[0], "jacobi_ppt": best[1], "jacobi_unroll": best[2],
-           "ms_per_step": best_t, "trials": trials}
+    shape = dict(block_size=best_build, jacobi_block=best[0], jacobi_ppt=best[1], jacobi_unroll=best[2])
+    plain = bool(params.plain_loads)
+    t = _time(scenes, params.replace(plain_loads=not plain, **shape), warm, steps)
+    trials.append({"plain_loads": not plain, "ms": t})
+    if verbose:
+        print("plain_loads", not plain, t)
+    if t < best_t:
+        plain, best_t = not plain, t
+    res = dict(shape, plain_loads=plain, ms_per_step=best_t, trials=trials)
     if use_cache:
         CACHE.parent.mkdir(parents=True, exist_ok=True)
         cache[key] = res
@@ -91,4 +101,5 @@ def autotune(scenes, params, warm=10, steps=20, use_cache=True, verbose=False) -
 
 def apply(params, tuned: dict):
     return params.replace(block_size=tuned["block_size"], jacobi_block=tuned["jacobi_block"],
-                          jacobi_ppt=tuned["jacobi_ppt"], jacobi_unroll=tuned["jacobi_unroll"])
+                          jacobi_ppt=tuned["jacobi_ppt"], jacobi_unroll=tuned["jacobi_unroll"],
+                          plain_loads=bool(tuned.get("plain_loads", params.plain_loads)))
