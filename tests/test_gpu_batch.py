@@ -100,5 +100,6 @@ def test_autotune_returns_valid_shape(tmp_path, monkeypatch):
     res = at.autotune(_scenes(), params, warm=3, steps=5)
     assert res["block_size"] in at.BUILD_BLOCKS
     assert (res["jacobi_block"], res["jacobi_ppt"], res["jacobi_unroll"]) in at.SOLVE_SHAPES
+    assert isinstance(res["plain_loads"], bool)
     again = at.autotune(_scenes(), params, warm=3, steps=5)
     assert again == res  # served from the cache
