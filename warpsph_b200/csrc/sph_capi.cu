@@ -1233,6 +1233,7 @@ int sph_neighbor_search(SphCtx* ctx) {
   StepAcc acc{};
   CK(cudaMemcpyAsync(&acc, ctx->acc, sizeof(StepAcc), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  if (acc.flags & SPH_F_TIMEOUT) return fail(ctx, SPH_E_TIMEOUT, "the cell sort's scan waited too long (SPH_F_TIMEOUT)");
   if (acc.flags & (SPH_F_FF_OVERFLOW | SPH_F_FB_OVERFLOW)) {
     rc = grow_capacity(ctx, acc.max_ff, acc.max_fb);
     if (rc) return rc;
