@@ -95,6 +95,31 @@ def test_full_size_reported_error_matches_terms(full_step):
     assert np.all(np.isfinite(out["x"])) and np.all(np.isfinite(out["v"])) and np.all(out["p"] >= 0)
 
 
+def test_full_size_runs_repeat_bit_for_bit():
+    """Two runs of the same 1M steps give the same words: the sort's order
+    is a function of the positions, every sum runs in list order, and the
+    solve's FP64 residual adds per-block partials in block order, so the
+    iteration counts and every state word repeat whatever the scheduling
+    (learned start with continuation, steps [0, 12), which include capped
+    solves)."""
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+    from warpsph_b200.solver import IISPH
+
+    scene = preset_scene("dam_break_1m")
+    runs = []
+    for _ in range(2):
+        params = preset_params("dam_break_1m", warm_start="mlp", warm_continue=True)
+        sol = IISPH(stage_path=None, params=params, scene=scene)
+        sol.steps(12)
+        hist = [(h["iterations"], h["avg_err"]) for h in sol.stats_history(12)]
+        runs.append((hist, sol.x.numpy(), sol.v.numpy(), sol.p.numpy()))
+        sol.close()
+    assert runs[0][0] == runs[1][0]
+    for a, b in zip(runs[0][1:], runs[1][1:]):
+        assert np.array_equal(a, b)
+
+
 def test_full_size_batch_of_64_matches_individual_runs():
     """The batched workload at full size: 64 dam breaks of 5k-200k particles
     (log-uniform, seeded) in one context with the learned warm start, against
