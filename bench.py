@@ -351,31 +351,31 @@ def bench_ours(args):
             traffic = ratio * sum(bytes_launch) / len(bytes_launch)
 
     # end to end through the C ABI with host buffers: every step uploads its
-    # input state (x, v, p) from pinned memory with sph_update_fluid (which,
-    # unlike sph_set_fluid, keeps the solver's history: the headline's
-    # continuation after capped solves runs as on the device), steps, and
-    # reads back x, v, p; every step's flags and v_max are checked
+    # input state (x, v: the reference's state) from pinned memory with
+    # sph_update_fluid (which, unlike sph_set_fluid, keeps the solver's
+    # history, the pressures included: the headline's continuation after
+    # capped solves runs as on the device), steps, and reads back x and v;
+    # every step's flags and v_max are checked
     s = fresh(headline)
     L, ctx = s._lib, s._ctx
     hx = torch.from_numpy(scene.fluid_x.copy()).pin_memory()
     hv = torch.from_numpy(scene.fluid_v.copy()).pin_memory()
-    hp = torch.zeros(n, dtype=torch.float32).pin_memory()
     stt = _lib.SphStepStats()
     vp = ctypes.c_void_p
     e2e_hist = []
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(K):
-        _lib.check(ctx, L.sph_update_fluid(ctx, vp(hx.data_ptr()), vp(hv.data_ptr()), vp(hp.data_ptr()), n))
+        _lib.check(ctx, L.sph_update_fluid(ctx, vp(hx.data_ptr()), vp(hv.data_ptr()), None, n))
         _lib.check(ctx, L.sph_step(ctx, ctypes.byref(stt)))
-        _lib.check(ctx, L.sph_get_fluid(ctx, vp(hx.data_ptr()), vp(hv.data_ptr()), vp(hp.data_ptr()), None, None))
+        _lib.check(ctx, L.sph_get_fluid(ctx, vp(hx.data_ptr()), vp(hv.data_ptr()), None, None, None))
         e2e_hist.append(stt.as_dict())
     e2e_s = time.perf_counter() - t0
     s.close()
     check_flags(e2e_hist)
     e2e_iters = int(sum(h["iterations"] for h in e2e_hist))
     e2e_value = world * K / ranks.max_over_ranks(e2e_s, dist, dev)
-    h2d = 28 * n
+    h2d = 24 * n
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -403,7 +403,7 @@ def bench_ours(args):
                          "bytes_rule": "per launch: iterations * (100 N + 8 P_ff) + 112 N"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": 28 * n + 80, "jacobi_iterations": e2e_iters,
+                    "d2h_bytes_per_step": 24 * n + 80, "jacobi_iterations": e2e_iters,
                     "call": "sph_update_fluid + sph_step + sph_get_fluid per step"},
             "gpu_launches": kernels_per_step(headline) * K,
             "clocks": clock,

@@ -140,6 +140,9 @@ int sph_set_fluid(SphCtx* ctx, const float* x3, const float* v3, int64_t n);
  * the state in host memory between steps (a checkpoint round trip, a coupled
  * host-side code): stepping on after sph_get_fluid + sph_update_fluid gives
  * the same result as stepping on directly.  n must equal the fluid count.
+ * p = NULL keeps the pressures on the device (the reference's state is x and
+ * v; the pressure is only the warm start's history), so a round trip of x
+ * and v alone also steps on exactly as the device would.
  * No counterpart in the reference, whose state lives in Warp arrays. */
 int sph_update_fluid(SphCtx* ctx, const float* x3, const float* v3, const float* p, int64_t n);
 

@@ -356,6 +356,34 @@ def test_deterministic_and_graph_equivalent():
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("with_p", [True, False])
+def test_host_round_trip_steps_on_exactly(with_p):
+    """sph_get_fluid then sph_update_fluid (x, v and p, or x and v with the
+    pressures kept on the device) between two steps changes nothing: the
+    run goes on bit for bit as without the round trip (learned start with
+    continuation after capped solves, so the pressure history matters)."""
+    from warpsph_b200.params import preset_params
+    from warpsph_b200.scenes import preset_scene
+
+    scene = preset_scene("dam_break_8k")
+    params = preset_params("dam_break_8k", warm_start="mlp", warm_continue=True)
+    outs = []
+    for trip in (False, True):
+        sol = _solver(params, scene)
+        sol.steps(3)
+        for _ in range(5):
+            if trip:
+                x, v, p = sol.x.numpy(), sol.v.numpy(), sol.p.numpy()
+                sol.update_state(x, v, p if with_p else None)
+            sol.step()
+        hist = [(h["iterations"], h["avg_err"], h["dt"]) for h in sol.stats_history(8)]
+        outs.append((hist, sol.x.numpy(), sol.v.numpy(), sol.p.numpy()))
+        sol.close()
+    assert outs[0][0] == outs[1][0]
+    for a, b in zip(outs[0][1:], outs[1][1:]):
+        assert np.array_equal(a, b)
+
+
 def test_texture_gathers_equal_plain_loads():
     """The solve's second pass (neighbour positions) and the neighbour
     build's second phase (positions, velocities) read through the texture

@@ -1022,8 +1022,8 @@ int sph_set_fluid(SphCtx* ctx, const float* x3, const float* v3, int64_t n) {
 }
 
 int sph_update_fluid(SphCtx* ctx, const float* x3, const float* v3, const float* p, int64_t n) {
-  if (!ctx || n != ctx->n || (n > 0 && (!x3 || !v3 || !p)))
-    return fail(ctx, SPH_E_INVALID, "sph_update_fluid replaces x, v and p of the current particles (n = fluid count)");
+  if (!ctx || n != ctx->n || (n > 0 && (!x3 || !v3)))
+    return fail(ctx, SPH_E_INVALID, "sph_update_fluid replaces x, v (and p) of the current particles (n = fluid count)");
   CK(cudaSetDevice(ctx->dev));
   if (n == 0) return SPH_OK;
   // the grid, dt, simulated time and the per-scene cap flags stay as they are
@@ -1032,7 +1032,10 @@ int sph_update_fluid(SphCtx* ctx, const float* x3, const float* v3, const float*
   float* sp = ctx->stage + 6 * n;
   CK(cudaMemcpyAsync(sx, x3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(sv, v3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemcpyAsync(sp, p, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
+  if (p) CK(cudaMemcpyAsync(sp, p, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
+  // p = NULL keeps each particle's pressure on the device: into original
+  // order before the pack below resets the state order
+  else CK(sph::launch_unsort1(int(n), ctx->orig_s, ctx->p_s, sp, ctx->stream));
   CK(sph::launch_pack_fluid(int(n), 0, sx, sv, ctx->pos_s, ctx->vel_s, ctx->orig_s, ctx->p_s, ctx->stream, sp));
   CK(cudaStreamSynchronize(ctx->stream));
   return SPH_OK;

@@ -175,14 +175,18 @@ class IISPH:
         self.n = len(x)
         _lib.check(self._ctx, self._lib.sph_set_fluid(self._ctx, _lib.ptr(x), _lib.ptr(v), self.n))
 
-    def update_state(self, x, v, p):
+    def update_state(self, x, v, p=None):
         """Replace positions, velocities and pressures (original order) of the
         current particles, keeping dt, time and the solver's history
-        (sph_update_fluid); set_state instead starts a new state."""
+        (sph_update_fluid); set_state instead starts a new state.  p=None
+        keeps the pressures on the device."""
         x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 3)
         v = np.ascontiguousarray(v, dtype=np.float32).reshape(-1, 3)
-        p = np.ascontiguousarray(p, dtype=np.float32).reshape(-1)
-        _lib.check(self._ctx, self._lib.sph_update_fluid(self._ctx, _lib.ptr(x), _lib.ptr(v), _lib.ptr(p), len(x)))
+        pp = None
+        if p is not None:
+            p = np.ascontiguousarray(p, dtype=np.float32).reshape(-1)
+            pp = _lib.ptr(p)
+        _lib.check(self._ctx, self._lib.sph_update_fluid(self._ctx, _lib.ptr(x), _lib.ptr(v), pp, len(x)))
 
     def add_fluid(self, x, v=None):
         """Append fluid particles (e.g. an emitter's new layer) to the state on
