@@ -127,9 +127,12 @@ def run_cpu_reference(budget_s: float, max_steps: int, nthreads: int = 0):
 
     The steps are timed one by one as they run, until K are done or the time
     budget is spent.  value = K / (timed seconds) when all K ran; otherwise
-    the remaining steps are charged at the mean time of the last timed steps
-    (past the start-up transient every step takes 2-6 iterations, which those
-    steps sample), and the line says how many were timed.  Iteration counts
+    the remaining steps are charged at the mean time of the last timed steps,
+    and the line says how many were timed.  That charge is a lower bound on
+    the CPU's time, so the value errs on the CPU's side: the last timed steps
+    of the 1M dam break take 2 iterations, while the p <- 0 solve averages
+    about 7 per step over steps [45, 500) (3784 iterations over [0, 500) on
+    the device, 681 of them in the first 45 steps).  Iteration counts
     are the oracle's own.  Two unit costs are reported beside it (a step with
     2 and one with 12 fixed iterations at the initial state), and the same
     2-iteration step on one thread."""
