@@ -264,7 +264,10 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Ker& ker) {
       // Learned warm-start inputs (kFeatures per particle, dimensionless; the
       // network standardises them with its own mean / std).  Pressures span
       // orders of magnitude, so they enter as asinh(p / (rho0 g h)).
-      float* f = a.feat + (long long)i * kFeatures;
+      // feature-major: feature c of sorted particle i at feat[c * feat_ld + i],
+      // so each of a warp's stores (and the network's loads) is one 128-byte row
+      float* f0 = a.feat + i;
+      auto f = [&](int c) -> float& { return f0[(long long)c * a.feat_ld]; };
       const float inv_rho0 = 1.0f / c.rho0;
       const float p_ref = 1.0f / (c.rho0 * c.gravity * c.h);  // 1 / (rho0 g h)
       const float h2 = c.h * c.h, h4 = h2 * h2;
@@ -272,21 +275,21 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Ker& ker) {
       if (aa > -c.inv_small && aa < c.inv_small) aa = (aa < 0.f ? -1.f : 1.f) * c.inv_small;
       const float p1 = fmaxf((c.rho0 - rho_adv) * c.omega / aa, 0.f);  // first Jacobi iterate from p = 0
       const float gx = sGx * c.m + Bx, gy = sGy * c.m + By, gz = sGz * c.m + Bz;  // grad rho
-      f[0] = rho_adv * inv_rho0 - 1.0f;                        // predicted density deviation
-      f[1] = (rho_adv - rho) * inv_rho0;                       // velocity divergence over the step
-      f[2] = aii * rr / (dt2 * c.m * c.m) * h4 * h4;           // a_ii in lattice units
-      f[3] = asinhf((a.pprev ? a.pprev[i] : 0.f) * p_ref);     // previous-step pressure
-      f[4] = float(cnt);                                       // fluid neighbour count
-      f[5] = sWb * inv_rho0;                                   // boundary psi sum (density share)
-      f[6] = sqrtf(gx * gx + gy * gy + gz * gz) * c.h * inv_rho0;  // |grad rho|
-      f[7] = asinhf(p1 * p_ref);                               // Jacobi source term
-      f[8] = gy * c.h * inv_rho0;                              // grad rho along gravity
-      f[9] = float(cntb);                                      // boundary neighbour count
+      f(0) = rho_adv * inv_rho0 - 1.0f;                        // predicted density deviation
+      f(1) = (rho_adv - rho) * inv_rho0;                       // velocity divergence over the step
+      f(2) = aii * rr / (dt2 * c.m * c.m) * h4 * h4;           // a_ii in lattice units
+      f(3) = asinhf((a.pprev ? a.pprev[i] : 0.f) * p_ref);     // previous-step pressure
+      f(4) = float(cnt);                                       // fluid neighbour count
+      f(5) = sWb * inv_rho0;                                   // boundary psi sum (density share)
+      f(6) = sqrtf(gx * gx + gy * gy + gz * gz) * c.h * inv_rho0;  // |grad rho|
+      f(7) = asinhf(p1 * p_ref);                               // Jacobi source term
+      f(8) = gy * c.h * inv_rho0;                              // grad rho along gravity
+      f(9) = float(cntb);                                      // boundary neighbour count
       // hydrostatic pressure of the fluid column above: depth below the
       // highest fluid particle of this grid column (x, z), in units of h
       const int3 top = make_int3(ci.x, 0, ci.z);
       const float depth = key_float(__ldg(a.coltop + fr.base + cell_index(g, top))) - xi.y;
-      f[10] = asinhf(fmaxf(depth, 0.f) / c.h);
+      f(10) = asinhf(fmaxf(depth, 0.f) / c.h);
     }
   }
   // bookkeeping: overflow flags, pair totals, max counts (once per step)

@@ -583,6 +583,7 @@ sph::BuildArgs build_args(SphCtx* ctx) {
   b.p0 = ctx->p_a;
   b.pos_q = ctx->pos_w;
   b.feat = (ctx->record_feat || ctx->P.warm_start == SPH_WARM_MLP) ? ctx->feat : nullptr;
+  b.feat_ld = ctx->n_cap;
   b.coltop = ctx->coltop;
   b.pos_tex = ctx->jac_tex ? (unsigned long long)ctx->pos_tex : 0ull;
   b.vel_tex = ctx->jac_tex ? (unsigned long long)ctx->vel_tex : 0ull;
@@ -621,6 +622,7 @@ int enqueue_warm(SphCtx* ctx) {
     m.n = ctx->n;
     m.w = ctx->mlp;
     m.feat = ctx->feat;
+    m.feat_ld = ctx->n_cap;  // feature-major, as the build writes them
     m.rho = ctx->rho;
     m.p_unit = float(ctx->P.rho0 * ctx->P.gravity * ctx->P.h);
     m.p0 = ctx->p_a;
@@ -1505,11 +1507,14 @@ int sph_get_features(SphCtx* ctx, float* feat, float* target) {
   std::vector<int> ow(n);
   CK(cudaMemcpy(ow.data(), ctx->orig_w, sizeof(int) * n, cudaMemcpyDeviceToHost));
   if (feat) {
-    std::vector<float> h(size_t(n) * sph::kFeatures);
-    CK(cudaMemcpy(h.data(), ctx->feat, sizeof(float) * h.size(), cudaMemcpyDeviceToHost));
-    for (int64_t k = 0; k < n; ++k)
-      std::memcpy(feat + size_t(ow[k]) * sph::kFeatures, h.data() + size_t(k) * sph::kFeatures,
-                  sizeof(float) * sph::kFeatures);
+    // device: feature-major over the sorted particles (leading dimension
+    // n_cap); out: rows of kFeatures in original order
+    std::vector<float> h(static_cast<size_t>(n));
+    for (int c = 0; c < sph::kFeatures; ++c) {
+      CK(cudaMemcpy(h.data(), ctx->feat + size_t(c) * size_t(ctx->n_cap), sizeof(float) * size_t(n),
+                    cudaMemcpyDeviceToHost));
+      for (int64_t k = 0; k < n; ++k) feat[size_t(ow[k]) * sph::kFeatures + c] = h[k];
+    }
   }
   if (target) {
     // the last step's converged pressure, in the state order of that step (= orig_w)

@@ -397,7 +397,8 @@ struct BuildArgs {
   float4* vadv;
   float* p0;               // initial pressure of the solve (p_1 for the zero warm start)
   float4* pos_q;           // the array `pos` points to: p0 / rho^2 goes into .w
-  float* feat;             // optional MLP feature rows (n x kFeatures), NULL to skip
+  float* feat;             // optional MLP inputs, feature-major (kFeatures x feat_ld), NULL to skip
+  long long feat_ld;       // feature c of sorted particle i at feat[c * feat_ld + i]
   const unsigned int* coltop;  // with feat: per grid column (x, z), the highest fluid y (ordered key)
   // texture objects over pos and vel (0: plain read-only loads): the second
   // phase's neighbour gathers, and (cand_tex) the first phase's candidates

@@ -49,7 +49,8 @@ struct MlpPacked {
 struct MlpInferArgs {
   long long n;
   const MlpPacked* w;
-  const float* feat;      // n x kFeatures, raw features
+  const float* feat;      // raw features: row-major n x kFeatures, or feature-major (feat_ld > 0)
+  long long feat_ld;      // > 0: feature c of row r at feat[c * feat_ld + r]
   const float* rho;
   float p_unit;           // rho0 g h: pressure of one target unit
   float* p0;              // out: initial pressure

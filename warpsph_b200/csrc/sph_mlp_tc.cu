@@ -209,12 +209,14 @@ __global__ void __launch_bounds__(kTile) k_mlp_infer_tc(MlpInferArgs a) {
 
   const long long tiles = (a.n + kTile - 1) / kTile;
   // the raw features of this thread's row of the next tile are loaded one
-  // tile ahead, so their latency overlaps the current tile's MMAs
+  // tile ahead, so their latency overlaps the current tile's MMAs; in the
+  // feature-major layout each of a warp's loads is one coalesced 128-byte row
   float fn[kFeatures];
+  const long long cs = a.feat_ld > 0 ? a.feat_ld : 1, rs = a.feat_ld > 0 ? 1 : kFeatures;
   auto load_row = [&](long long tile) {
     const long long r = tile * kTile + tid;
 #pragma unroll
-    for (int c = 0; c < kFeatures; ++c) fn[c] = (tile < tiles && r < a.n) ? __ldg(a.feat + r * kFeatures + c) : 0.f;
+    for (int c = 0; c < kFeatures; ++c) fn[c] = (tile < tiles && r < a.n) ? __ldg(a.feat + c * cs + r * rs) : 0.f;
   };
   load_row(blockIdx.x);
   for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
