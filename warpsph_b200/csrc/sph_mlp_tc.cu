@@ -211,12 +211,16 @@ __global__ void __launch_bounds__(kTile) k_mlp_infer_tc(MlpInferArgs a) {
   // the raw features of this thread's row of the next tile are loaded one
   // tile ahead, so their latency overlaps the current tile's MMAs; in the
   // feature-major layout each of a warp's loads is one coalesced 128-byte row
-  float fn[kFeatures];
+  // (with the row's density and previous pressure, read by the epilogue)
+  float fn[kFeatures], rho_n = 1.f, pprev_n = 0.f;
   const long long cs = a.feat_ld > 0 ? a.feat_ld : 1, rs = a.feat_ld > 0 ? 1 : kFeatures;
   auto load_row = [&](long long tile) {
     const long long r = tile * kTile + tid;
+    const bool ok = tile < tiles && r < a.n;
 #pragma unroll
-    for (int c = 0; c < kFeatures; ++c) fn[c] = (tile < tiles && r < a.n) ? __ldg(a.feat + c * cs + r * rs) : 0.f;
+    for (int c = 0; c < kFeatures; ++c) fn[c] = ok ? __ldg(a.feat + c * cs + r * rs) : 0.f;
+    if (a.p0) rho_n = ok ? __ldg(a.rho + r) : 1.f;
+    if (a.pprev) pprev_n = ok ? __ldg(a.pprev + r) : 0.f;
   };
   load_row(blockIdx.x);
   for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
@@ -225,6 +229,7 @@ __global__ void __launch_bounds__(kTile) k_mlp_infer_tc(MlpInferArgs a) {
     // the residual's base, unrounded: the larger of asinh(p_prev / (rho0 g h))
     // and asinh(depth / h), the hydrostatic pressure of the column above
     const float u_prev = fmaxf(fn[3], fn[10]);
+    const float rho_row = rho_n, pprev_row = pprev_n;
     // 1. standardised features of this row, BF16, K padded to 16 with zeros
     {
       float f[kIn];
@@ -311,11 +316,10 @@ __global__ void __launch_bounds__(kTile) k_mlp_infer_tc(MlpInferArgs a) {
       if (a.p0) {
         const int sc = a.scenes ? find_scene(a.scenes->fluid_off, a.scenes->nscenes, int(row)) : 0;
         const float p = (a.restart && __ldg(a.restart + sc))
-                            ? __ldg(a.pprev + row)
+                            ? pprev_row
                             : sinhf(fmaxf(u_prev + fminf(y * s.t_scale, kMaxRise), 0.f)) * a.p_unit;
-        const float rho = __ldg(a.rho + row);
         a.p0[row] = p;
-        reinterpret_cast<float*>(a.pos_q + row)[3] = p / (rho * rho);
+        reinterpret_cast<float*>(a.pos_q + row)[3] = p / (rho_row * rho_row);
       }
       if (a.pred) a.pred[row] = y;
     }
