@@ -311,6 +311,8 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Ker& ker) {
 
 // Highest fluid y of each grid column (x, z): every sorted fluid particle
 // raises the key of its column's bottom cell (cy = 0).
+// Sorted neighbours usually share a column, so the lanes of a warp that do
+// combine their keys first and one of them updates the column.
 __global__ void k_column_top(BuildArgs a, unsigned int* coltop) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
@@ -318,7 +320,10 @@ __global__ void k_column_top(BuildArgs a, unsigned int* coltop) {
   const float4 xi = a.pos[i];
   int3 c = cell_coord(fr.g, xi.x, xi.y, xi.z);
   c.y = 0;
-  atomicMax(coltop + fr.base + cell_index(fr.g, c), float_key(xi.y));
+  const int col = fr.base + cell_index(fr.g, c);
+  const unsigned int same = __match_any_sync(__activemask(), col);
+  const unsigned int key = __reduce_max_sync(same, float_key(xi.y));
+  if ((threadIdx.x & 31) == unsigned(__ffs(same) - 1)) atomicMax(coltop + col, key);
 }
 
 cudaError_t launch_column_top(const BuildArgs& a, unsigned int* coltop, int total_cells, cudaStream_t s) {
