@@ -61,6 +61,7 @@ struct SphCtx {
   int64_t n = 0, n_cap = 0;
   int K_ff = 0, K_fb = 0;
   float4 *pos_s = nullptr, *vel_s = nullptr, *pos_w = nullptr, *vel_w = nullptr;
+  float2* yz_w = nullptr;  // (y, z) of pos_w: pass B's compact position gathers
   int *orig_s = nullptr, *orig_w = nullptr;
   float *p_s = nullptr, *pprev_w = nullptr;
   int *key = nullptr, *rank = nullptr, *sort_src = nullptr, *sort_orig = nullptr;
@@ -89,6 +90,7 @@ struct SphCtx {
   bool jac_tex = false;                               // pass B reads x_j through the texture path
   cudaTextureObject_t pos_tex = 0;                    // over pos_w, when jac_tex
   cudaTextureObject_t vel_tex = 0;                    // over vel_w, when jac_tex
+  cudaTextureObject_t yz_tex = 0;                     // over yz_w, when jac_tex
   int stall_block = -1;                               // sph_test_stall_barrier
   int withhold_mma = 0;                               // sph_test_withhold_mma
   int chunk = 256;                                    // particles per solve chunk
@@ -242,15 +244,49 @@ Grid fit_grid(const SphParams& P, const double* lo, const double* hi) {
 
 int upload_scene_table(SphCtx* ctx) {
   const int S = ctx->S;
-  // scene-aligned chunks of at most kChunk fluid slots
+  // Scene-aligned chunks of at most ctx->chunk fluid slots, warp-aligned, and
+  // as many of them as the persistent grid takes in whole rounds: the blocks
+  // take chunks round-robin, so with ceil(n / chunk) full chunks the blocks
+  // holding one chunk more set every pass's length.  Each scene's warps are
+  // spread evenly over its share of rounds * grid chunks instead (chunks of
+  // w or w + 1 warps), so every block ends a pass with the same work.
   std::vector<int2> chunks;
   std::vector<int> cscene;
   sph::SceneTable T{};
   T.nscenes = S;
+  const int64_t wchunk = std::max<int64_t>(1, ctx->chunk / 32);
+  std::vector<int64_t> ws(S), ms(S, 0);
+  int64_t warps_tot = 0;
+  for (int sc = 0; sc < S; ++sc) warps_tot += ws[sc] = (ctx->f_off[sc + 1] - ctx->f_off[sc] + 31) / 32;
+  const int64_t grid = std::max(1, ctx->coop_grid);
+  const int64_t target = grid * std::max<int64_t>(1, ((warps_tot + wchunk - 1) / wchunk + grid - 1) / grid);
+  // each scene's share of the target chunk count (largest remainders round
+  // up), at least enough for chunks of at most wchunk warps, at most one
+  // chunk per warp
+  std::vector<std::pair<int64_t, int>> rem;
+  int64_t left = target;
+  for (int sc = 0; sc < S; ++sc) {
+    if (ws[sc] == 0) continue;
+    ms[sc] = std::min(ws[sc], std::max(ws[sc] * target / warps_tot, (ws[sc] + wchunk - 1) / wchunk));
+    left -= ms[sc];
+    rem.emplace_back(ws[sc] * target % warps_tot, -sc);
+  }
+  std::sort(rem.rbegin(), rem.rend());
+  for (const auto& r : rem) {
+    if (left <= 0) break;
+    const int sc = -r.second;
+    if (ms[sc] < ws[sc]) {
+      ++ms[sc];
+      --left;
+    }
+  }
   for (int sc = 0; sc < S; ++sc) {
     T.chunk_off[sc] = int(chunks.size());
-    for (int64_t a = ctx->f_off[sc]; a < ctx->f_off[sc + 1]; a += ctx->chunk) {
-      chunks.push_back(make_int2(int(a), int(std::min<int64_t>(a + ctx->chunk, ctx->f_off[sc + 1]))));
+    const int64_t a0 = ctx->f_off[sc], a1 = ctx->f_off[sc + 1];
+    const int64_t w = ws[sc], m = ms[sc];
+    for (int64_t k = 0; k < m; ++k) {
+      const int64_t b = a0 + 32 * (k * w / m), e = std::min(a1, a0 + 32 * ((k + 1) * w / m));
+      chunks.push_back(make_int2(int(b), int(e)));
       cscene.push_back(sc);
     }
   }
@@ -467,7 +503,7 @@ constexpr bool kBuildTexCandidates = false;
 // 1-D texture objects over the work arrays of positions and velocities
 // (float4 per slot): read-only gathers that then use the texture path.
 int make_textures(SphCtx* ctx) {
-  for (cudaTextureObject_t* t : {&ctx->pos_tex, &ctx->vel_tex})
+  for (cudaTextureObject_t* t : {&ctx->pos_tex, &ctx->vel_tex, &ctx->yz_tex})
     if (*t) {
       cudaDestroyTextureObject(*t);
       *t = 0;
@@ -483,6 +519,14 @@ int make_textures(SphCtx* ctx) {
     td.readMode = cudaReadModeElementType;
     CK(cudaCreateTextureObject(k == 0 ? &ctx->pos_tex : &ctx->vel_tex, &rd, &td, nullptr));
   }
+  cudaResourceDesc rd{};
+  rd.resType = cudaResourceTypeLinear;
+  rd.res.linear.devPtr = ctx->yz_w;
+  rd.res.linear.desc = cudaCreateChannelDesc<float2>();
+  rd.res.linear.sizeInBytes = sizeof(float2) * size_t(ctx->n_cap);
+  cudaTextureDesc td{};
+  td.readMode = cudaReadModeElementType;
+  CK(cudaCreateTextureObject(&ctx->yz_tex, &rd, &td, nullptr));
   return SPH_OK;
 }
 
@@ -494,6 +538,7 @@ int alloc_fluid(SphCtx* ctx, int64_t n) {
   CK(dalloc(ctx->vel_s, m));
   CK(dalloc(ctx->pos_w, m));
   CK(dalloc(ctx->vel_w, m));
+  CK(dalloc(ctx->yz_w, m));
   {
     const int rc = make_textures(ctx);
     if (rc) return rc;
@@ -600,7 +645,7 @@ int enqueue_front(SphCtx* ctx) {
   }
   CK(sph::launch_sort(fluid_sort_args(ctx), ctx->total_cells, ctx->stream));
   CK(sph::launch_gather(int(ctx->n), ctx->sort_src, ctx->sort_orig, ctx->pos_s, ctx->vel_s, ctx->p_s, ctx->pos_w,
-                        ctx->vel_w, ctx->orig_w, ctx->pprev_w, ctx->stream));
+                        ctx->vel_w, ctx->orig_w, ctx->pprev_w, ctx->stream, ctx->jac_tex ? ctx->yz_w : nullptr));
   int block = ctx->P.block_size > 0 ? ctx->P.block_size : 128;
   const sph::BuildArgs b = build_args(ctx);
   if (b.feat) CK(sph::launch_column_top(b, ctx->coltop, ctx->total_cells, ctx->stream));
@@ -686,7 +731,7 @@ int enqueue_jacobi(SphCtx* ctx) {
   // 0.5 p_prev start runs the reference's extra Ap_0 evaluation (pass 0).
   j.start_iter = (ctx->P.warm_start == SPH_WARM_HALF) ? 0 : 1;
   j.grad_spline = ctx->g_spline ? 1 : 0;
-  j.xtex = (ctx->jac_tex && ctx->g_spline) ? (unsigned long long)ctx->pos_tex : 0ull;
+  j.yztex = (ctx->jac_tex && ctx->g_spline) ? (unsigned long long)ctx->yz_tex : 0ull;
   j.budget = (long long)ctx->P.timeout_ms * (long long)ctx->clock_khz;
   j.stall_block = ctx->stall_block;
   j.dt_max = ctx->P.dt_max;
@@ -904,9 +949,10 @@ void sph_destroy(SphCtx* ctx) {
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   if (ctx->pos_tex) cudaDestroyTextureObject(ctx->pos_tex);
   if (ctx->vel_tex) cudaDestroyTextureObject(ctx->vel_tex);
+  if (ctx->yz_tex) cudaDestroyTextureObject(ctx->yz_tex);
   void* ptrs[] = {ctx->d_w, ctx->d_g, ctx->bpos, ctx->bvel, ctx->borig, ctx->bpos_t, ctx->bvel_t, ctx->borig_t,
                   ctx->bkey, ctx->brank, ctx->bsrc, ctx->bcell_start, ctx->pos_s, ctx->vel_s,
-                  ctx->pos_w, ctx->vel_w, ctx->orig_s, ctx->orig_w, ctx->p_s, ctx->pprev_w, ctx->key, ctx->rank,
+                  ctx->pos_w, ctx->vel_w, ctx->yz_w, ctx->orig_s, ctx->orig_w, ctx->p_s, ctx->pprev_w, ctx->key, ctx->rank,
                   ctx->sort_src, ctx->sort_orig, ctx->cell_count, ctx->cell_start, ctx->scan_part, ctx->scan_status, ctx->coltop, ctx->nbr_ff,
                   ctx->cnt_ff, ctx->nbr_fb, ctx->cnt_fb, ctx->rho, ctx->bvec, ctx->dii_aii, ctx->vadv, ctx->a4,
                   ctx->p_a, ctx->p_b, ctx->Ap, ctx->pmlp, ctx->feat, ctx->p_start, ctx->mlp, ctx->stage, ctx->partials, ctx->st, ctx->acc, ctx->ring,
@@ -946,6 +992,10 @@ int sph_set_tables(SphCtx* ctx, const float* w, int32_t nw, const float* g, int3
   if (b != ctx->blocks_per_sm) {
     ctx->blocks_per_sm = b;
     ctx->coop_grid = b * ctx->sm_count;
+    if (ctx->grid_valid) {
+      rc = upload_scene_table(ctx);  // chunks are cut for the grid size
+      if (rc) return rc;
+    }
   }
   if (ctx->nb) return sort_boundary(ctx);  // psi depends on W
   return SPH_OK;

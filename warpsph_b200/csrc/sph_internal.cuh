@@ -433,7 +433,7 @@ struct JacobiArgs {
   const int* orig_w;
   float* p_a;              // ping
   float* p_b;              // pong
-  float4* a4;              // (d_ii p + s, 0): dt^2 times the pressure acceleration
+  float4* a4;              // (d_ii p + s, x): dt^2 times the pressure acceleration, and x of the position
   float* Ap;
   Partial* partials;       // one per chunk
   DevState* st;
@@ -450,7 +450,8 @@ struct JacobiArgs {
   float* p_out;
   int start_iter;          // 1: p_1 came from the build; 0: warm start, run pass 0
   int grad_spline;         // 1: the gradient table is the cubic spline's (closed form in the passes)
-  unsigned long long xtex; // texture object over pos (0: none): pass B fetches x_j through the texture path
+  unsigned long long yztex; // texture object over (y, z) of pos (0: none): pass B then takes x_j from a4's .w
+                            // and fetches (y_j, z_j) through the texture path
   long long budget;        // barrier spin budget in SM cycles
   int stall_block;         // test hook: this block skips its first barrier arrival (-1: none)
   double dt_max, cfl_len, inv_small_d, eta_d;
@@ -480,7 +481,7 @@ cudaError_t launch_psi(const PsiArgs& a, int block, cudaStream_t s);
 cudaError_t launch_psi_sorted(const PsiArgs& a, float* psi_sorted, int block, cudaStream_t s);
 cudaError_t launch_gather(int n, const int* sort_src, const int* sort_orig, const float4* pos_in,
                           const float4* vel_in, const float* p_in, float4* pos_out, float4* vel_out,
-                          int* orig_out, float* p_out, cudaStream_t s);
+                          int* orig_out, float* p_out, cudaStream_t s, float2* yz_out = nullptr);
 bool jacobi_variant_ok(int block, int ppt, int unroll);
 cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, bool spline, int* blocks_per_sm, size_t* smem,
                           bool tex = false);

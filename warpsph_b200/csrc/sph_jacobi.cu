@@ -52,19 +52,17 @@ namespace sph {
 // resident instead of the list stream.  pos (its .w) and a4 are rewritten
 // between barriers, so they are read with plain coherent loads.  NG = 1
 // gathers pos only, NG = 2 also the second array.
-// Positions of neighbours: plain coherent loads, or (XT) fetches through the
-// texture path from a texture object over the same array, which only pass B
-// uses (it reads x_j, which the solve never changes, and not .w).
-template <bool XT>
-__device__ __forceinline__ float4 load_pos(const float4* pos, unsigned long long tex, int j) {
-  if (XT) return tex1Dfetch<float4>(cudaTextureObject_t(tex), j);
-  return pos[j];
-}
-
-template <int kUnroll, int NG, bool XT = false, typename Body>
+// NG = 3 is pass B's compact form: the second array is a4, whose .w holds the
+// neighbour's x (pass A stores it there), and (y_j, z_j) come as an 8-byte
+// record through the texture path from a texture object over a (y, z) copy of
+// the positions, written by the cell sort's gather before the solve (the solve
+// never changes positions, so the texture path sees no stale data).  Pass B
+// then moves 24 bytes per neighbour instead of 32, and the 8-byte records put
+// a warp's gathers on fewer lines.
+template <int kUnroll, int NG, typename Body>
 __device__ __forceinline__ void for_neighbours(const int* __restrict__ nb, int cnt, int self,
                                                const float4* pos, const float4* other, Body body,
-                                               unsigned long long xtex = 0) {
+                                               unsigned long long yztex = 0) {
   const int wmax = __reduce_max_sync(0xffffffffu, cnt);
   int jn[kUnroll];
 #pragma unroll
@@ -80,11 +78,21 @@ __device__ __forceinline__ void for_neighbours(const int* __restrict__ nb, int c
     float4 xj[kUnroll], oj[kUnroll];
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
-      xj[u] = load_pos<XT>(pos, xtex, j[u]);
-      if (NG == 2) oj[u] = other[j[u]];
+      if (NG == 3) {
+        oj[u] = other[j[u]];
+        const float2 yz = tex1Dfetch<float2>(cudaTextureObject_t(yztex), j[u]);
+        xj[u].y = yz.x;
+        xj[u].z = yz.y;
+      } else {
+        xj[u] = pos[j[u]];
+        if (NG == 2) oj[u] = other[j[u]];
+      }
     }
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) body(xj[u], oj[u]);
+    for (int u = 0; u < kUnroll; ++u) {
+      if (NG == 3) xj[u].x = oj[u].w;
+      body(xj[u], oj[u]);
+    }
   }
 }
 
@@ -110,7 +118,7 @@ __device__ inline void pass_a(int i, bool live, const JacobiArgs& a, const Tab& 
   if (!live) return;
   const float4 da = __ldg(a.dii_aii + i);
   const float p = pc[i];
-  a.a4[i] = make_float4(da.x * p + (-t3 * sx), da.y * p + (-t3 * sy), da.z * p + (-t3 * sz), 0.f);
+  a.a4[i] = make_float4(da.x * p + (-t3 * sx), da.y * p + (-t3 * sy), da.z * p + (-t3 * sz), xi.x);
 }
 
 // pass B for particle i: Ap (compute_term_Ap_2, IISPH.py:469-518), the density
@@ -124,11 +132,11 @@ __device__ inline void pass_b(int i, bool live, const JacobiArgs& a, const Tab& 
   const int cnt = live ? min(__ldg(a.cnt_ff + i), c.max_ff) : 0;
   const int* nb = a.nbr_ff + ell_index(i, 0, c.max_ff);
   float acc = 0.f;
-  for_neighbours<U, 2, XT>(nb, cnt, i, a.pos, a.a4, [&](const float4 xj, const float4 aj) {
+  for_neighbours<U, XT ? 3 : 2>(nb, cnt, i, a.pos, a.a4, [&](const float4 xj, const float4 aj) {
     const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
     const float gs = G(c, dx * dx + dy * dy + dz * dz);
     acc = fmaf(gs, (ai.x - aj.x) * dx + (ai.y - aj.y) * dy + (ai.z - aj.z) * dz, acc);
-  }, a.xtex);
+  }, a.yztex);
   if (!live) return;
   const float4 bv = __ldg(a.bvec + i);
   const float4 da = __ldg(a.dii_aii + i);
@@ -532,7 +540,7 @@ cudaError_t jacobi_config(int block, int ppt, int unroll, int sg, bool spline, i
 
 cudaError_t launch_jacobi(const JacobiArgs& a, int grid, int block, int ppt, int unroll, size_t smem,
                           cudaStream_t s) {
-  JacobiKernel k = jacobi_kernel(grad_mode(a.c.sg, a.grad_spline != 0, a.xtex != 0), block, ppt, unroll);
+  JacobiKernel k = jacobi_kernel(grad_mode(a.c.sg, a.grad_spline != 0, a.yztex != 0), block, ppt, unroll);
   if (!k) return cudaErrorInvalidValue;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);

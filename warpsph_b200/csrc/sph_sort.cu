@@ -278,11 +278,14 @@ __global__ void k_cell_sort(const int* __restrict__ start, int ncells, int* src,
 __global__ void k_gather(int n, const int* __restrict__ sort_src, const int* __restrict__ sort_orig,
                          const float4* __restrict__ pos_in, const float4* __restrict__ vel_in,
                          const float* __restrict__ p_in, float4* __restrict__ pos_out,
-                         float4* __restrict__ vel_out, int* __restrict__ orig_out, float* __restrict__ p_out) {
+                         float4* __restrict__ vel_out, int* __restrict__ orig_out, float* __restrict__ p_out,
+                         float2* __restrict__ yz_out) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   int s = sort_src[k];
-  pos_out[k] = pos_in[s];
+  const float4 x = pos_in[s];
+  pos_out[k] = x;
+  if (yz_out) yz_out[k] = make_float2(x.y, x.z);
   if (vel_out) vel_out[k] = vel_in[s];
   orig_out[k] = sort_orig[k];
   if (p_out) p_out[k] = p_in[s];
@@ -310,11 +313,11 @@ cudaError_t launch_sort(const SortArgs& a, int ncells, cudaStream_t s) {
 
 cudaError_t launch_gather(int n, const int* sort_src, const int* sort_orig, const float4* pos_in,
                           const float4* vel_in, const float* p_in, float4* pos_out, float4* vel_out,
-                          int* orig_out, float* p_out, cudaStream_t s) {
+                          int* orig_out, float* p_out, cudaStream_t s, float2* yz_out) {
   if (n <= 0) return cudaSuccess;
   const int T = 256;
   k_gather<<<(n + T - 1) / T, T, 0, s>>>(n, sort_src, sort_orig, pos_in, vel_in, p_in, pos_out, vel_out,
-                                        orig_out, p_out);
+                                        orig_out, p_out, yz_out);
   return cudaGetLastError();
 }
 
