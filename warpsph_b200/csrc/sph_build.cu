@@ -174,6 +174,19 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Ker& ker) {
     // the neighbours' velocities through the texture path only when they
     // are the step's velocities (not the v_adv the viscosity pass wrote)
     const unsigned long long vtex = (MODE == kBuildAdvect) ? 0ull : a.vel_tex;
+    // compact form: (v_j, x_j) from the velocity record and (y_j, z_j) from
+    // the 8-byte copy, 24 bytes per neighbour instead of two 16-byte records
+    const unsigned long long yztex = (MODE == kBuildAdvect) ? 0ull : a.yz_tex;
+    auto load = [&](int j, float4& xj, float4& vj) {
+      if (yztex) {
+        vj = tex1Dfetch<float4>(cudaTextureObject_t(vtex), j);
+        const float2 yz = tex1Dfetch<float2>(cudaTextureObject_t(yztex), j);
+        xj = make_float4(vj.w, yz.x, yz.y, 0.f);
+      } else {
+        xj = ro_load(a.pos, a.pos_tex, j);
+        vj = ro_load(vsrc, vtex, j);
+      }
+    };
     int k = 0;
     for (; k + 4 <= nf; k += 4) {
       int j[4];
@@ -181,16 +194,14 @@ __device__ __forceinline__ void build_body(const BuildArgs& a, const Ker& ker) {
 #pragma unroll
       for (int u = 0; u < 4; ++u) j[u] = nbr[(k + u) * kWarp];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        xj[u] = ro_load(a.pos, a.pos_tex, j[u]);
-        vj[u] = ro_load(vsrc, vtex, j[u]);
-      }
+      for (int u = 0; u < 4; ++u) load(j[u], xj[u], vj[u]);
 #pragma unroll
       for (int u = 0; u < 4; ++u) fluid(xj[u], vj[u]);
     }
     for (; k < nf; ++k) {
-      const int j = nbr[k * kWarp];
-      fluid(ro_load(a.pos, a.pos_tex, j), ro_load(vsrc, vtex, j));
+      float4 xj, vj;
+      load(nbr[k * kWarp], xj, vj);
+      fluid(xj, vj);
     }
 
     float sWb = 0.f, Bx = 0.f, By = 0.f, Bz = 0.f, divb = 0.f;

@@ -633,6 +633,7 @@ sph::BuildArgs build_args(SphCtx* ctx) {
   b.pos_tex = ctx->jac_tex ? (unsigned long long)ctx->pos_tex : 0ull;
   b.vel_tex = ctx->jac_tex ? (unsigned long long)ctx->vel_tex : 0ull;
   b.cand_tex = kBuildTexCandidates ? b.pos_tex : 0ull;
+  b.yz_tex = ctx->jac_tex ? (unsigned long long)ctx->yz_tex : 0ull;
   return b;
 }
 

@@ -403,6 +403,9 @@ struct BuildArgs {
   // texture objects over pos and vel (0: plain read-only loads): the second
   // phase's neighbour gathers, and (cand_tex) the first phase's candidates
   unsigned long long pos_tex, vel_tex, cand_tex;
+  // texture object over the (y, z) copy of pos (0: none); when set, vel's .w
+  // holds x and the second phase gathers (v, x) and (y, z) instead of pos and v
+  unsigned long long yz_tex;
 };
 
 // Order-preserving uint key of a float (atomicMax on keys = max on floats);

@@ -286,7 +286,13 @@ __global__ void k_gather(int n, const int* __restrict__ sort_src, const int* __r
   const float4 x = pos_in[s];
   pos_out[k] = x;
   if (yz_out) yz_out[k] = make_float2(x.y, x.z);
-  if (vel_out) vel_out[k] = vel_in[s];
+  if (vel_out) {
+    float4 v = vel_in[s];
+    // with the (y, z) copy, the velocity record carries x in its .w: the
+    // build then gathers a neighbour's position and velocity as 24 bytes
+    if (yz_out) v.w = x.x;
+    vel_out[k] = v;
+  }
   orig_out[k] = sort_orig[k];
   if (p_out) p_out[k] = p_in[s];
 }
