@@ -461,6 +461,7 @@ static cudaError_t launch_build_mode(const BuildArgs& a, int grid, int block, cu
             cudaFuncSetAttribute(k_build<true, MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
       }
+      prefer_l1(k_build<true, MODE, true>, block, smem);
       k_build<true, MODE, true><<<grid, block, smem, s>>>(a);
     } else {
       k_build<false, MODE, true><<<grid, block, 0, s>>>(a);
@@ -472,6 +473,7 @@ static cudaError_t launch_build_mode(const BuildArgs& a, int grid, int block, cu
           cudaFuncSetAttribute(k_build<true, MODE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
       if (e != cudaSuccess) return e;
     }
+    prefer_l1(k_build<true, MODE, false>, block, smem);
     k_build<true, MODE, false><<<grid, block, smem, s>>>(a);
   } else {
     k_build<false, MODE, false><<<grid, block, 0, s>>>(a);

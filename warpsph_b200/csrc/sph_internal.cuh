@@ -471,6 +471,32 @@ struct PsiArgs {
   int w0_from_table;       // 1: W(0) is read from w_table[0] on the device instead of c.w0
 };
 
+// Shared-memory carveout hint for a kernel that reads its neighbours through
+// the L1: the smallest share of the SM's unified L1 / shared storage that
+// still holds every block the registers and threads allow, so the rest stays
+// L1.  Left to itself the driver gave the build's 8 blocks of 9 KB a 132 KB
+// carveout (about 120 KB of L1); with the hint it takes 100 KB.  The solve
+// does not use it: for its 4 blocks of 1.2 KB the driver answered the hint
+// with 64 KB where it picks 16 KB by itself.  A hint only: errors are
+// cleared and ignored.
+template <class Kernel>
+inline void prefer_l1(Kernel* k, int block, size_t dyn_smem) {
+  int dev = 0, per_sm = 0, reserved = 0, nb = 0;
+  cudaFuncAttributes fa{};
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaFuncGetAttributes(&fa, k) != cudaSuccess ||
+      cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, block, dyn_smem) != cudaSuccess || per_sm <= 0) {
+    cudaGetLastError();
+    return;
+  }
+  const size_t need = size_t(nb) * (fa.sharedSizeBytes + dyn_smem + size_t(reserved));
+  size_t pct = (100 * need + size_t(per_sm) - 1) / size_t(per_sm);
+  if (pct > 100) pct = 100;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, int(pct)) != cudaSuccess)
+    cudaGetLastError();
+}
+
 // launchers (host)
 cudaError_t launch_sort(const SortArgs& a, int ncells, cudaStream_t s);
 // neighbour-build passes: one fused pass without viscosity, or lists + rho,
