@@ -4,7 +4,12 @@
 //   pos  float4 (x, y, z, q)          vel  float4 (vx, vy, vz, 0)
 //        q = p / rho^2 of the current pressure iterate in the solve's work
 //        array (first written by the build or the warm-start network, then by
-//        every Jacobi update); the step's state arrays carry 0 there
+//        every Jacobi update); the step's state arrays carry 0 there.  With
+//        the texture path on, the work copy of vel carries x in .w and a
+//        float2 (y, z) copy of pos sits beside it: the build's second phase
+//        and the solve's pass B gather a position as (x from a 16-byte record
+//        they read anyway) + 8 bytes
+//   a4   float4 (a, x)                a = d_ii p + s of the current iterate
 //   bpos float4 (x, y, z, psi)        boundary, sorted once
 //   nbr  int32, tile-major ELL: element k of particle i sits at
 //        (i/32)*32*K + k*32 + i%32, so a warp reading its k-th neighbours
