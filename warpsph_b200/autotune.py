@@ -29,7 +29,7 @@ CACHE = Path(os.environ.get("WPSPH_AUTOTUNE_CACHE", Path.home() / ".cache" / "wa
 def _signature(scenes, params) -> str:
     n = sum(s.n for s in scenes)
     nb = sum(s.boundary_n for s in scenes)
-    return f"scenes={len(scenes)},n={n},nb={nb},d={params.diameter},warm={params.warm_start},v2"
+    return f"scenes={len(scenes)},n={n},nb={nb},d={params.diameter},warm={params.warm_start},v3"
 
 
 def _time(scenes, params, warm, steps) -> float:
@@ -74,7 +74,10 @@ def autotune(scenes, params, warm=10, steps=20, use_cache=True, verbose=False) -
             print("build", bb, t)
         if t < best_t:
             best_build, best_t = bb, t
-    best = (256, 1, 2)
+    # the build sweep ran the solve at the caller's shape (the library's
+    # default where unset), so best_t is that shape's time: a solve shape must
+    # beat it to replace it
+    best = (params.jacobi_block or 256, params.jacobi_ppt or 1, params.jacobi_unroll or 4)
     for blk, ppt, unr in SOLVE_SHAPES:
         t = _time(scenes, params.replace(block_size=best_build, jacobi_block=blk, jacobi_ppt=ppt,
                                          jacobi_unroll=unr), warm, steps)
