@@ -75,7 +75,9 @@ typedef struct SphParams {
   int32_t device;        /* CUDA device ordinal */
   int32_t block_size;    /* threads per block of the neighbour build (0 = 128) */
   int32_t timeout_ms;    /* bound on every grid-wide wait */
-  int32_t jacobi_block;  /* threads per block of the pressure solve: 128 or 256 (0 = 256) */
+  int32_t jacobi_block;  /* threads per block of the pressure solve: 128 or 256 with any
+                            (jacobi_ppt, jacobi_unroll) below, or 512 / 1024 with (1, 4)
+                            (0 = 1024) */
   int32_t jacobi_ppt;    /* particles per solve thread: 1 or 2 (0 = 1) */
   int32_t jacobi_unroll; /* neighbour-loop unroll of the solve: 2, 4 or 8 (0 = 4) */
   int32_t move_boundary;  /* 1: boundary particles move with their velocities, x += v dt after

@@ -25,19 +25,23 @@ def _run(monkeypatch, tmp_path, cost, params=None):
 
 
 def _shape(p):
-    return (p.jacobi_block or 256, p.jacobi_ppt or 1, p.jacobi_unroll or 4)
+    return (p.jacobi_block or at.DEFAULT_SOLVE[0], p.jacobi_ppt or at.DEFAULT_SOLVE[1],
+            p.jacobi_unroll or at.DEFAULT_SOLVE[2])
 
 
 def test_default_solve_shape_kept_when_nothing_beats_it(monkeypatch, tmp_path):
-    # the build sweep (solve at the default 256, 1, 4) is fastest; every solve
-    # shape is slower, (256, 1, 2) the slowest: the default must come back
+    # the build sweep (solve at the library's default shape) is fastest; every
+    # other solve shape is slower, (256, 1, 2) the slowest: the default must
+    # come back, not (256, 1, 2)
     def cost(p):
         if p.jacobi_block == 0:
+            return 1.0
+        if _shape(p) == at.DEFAULT_SOLVE:
             return 1.0
         return 3.0 if _shape(p) == (256, 1, 2) else 1.0 + 0.01 * p.jacobi_unroll
 
     res, _ = _run(monkeypatch, tmp_path, cost)
-    assert (res["jacobi_block"], res["jacobi_ppt"], res["jacobi_unroll"]) == (256, 1, 4)
+    assert (res["jacobi_block"], res["jacobi_ppt"], res["jacobi_unroll"]) == at.DEFAULT_SOLVE
     assert res["ms_per_step"] == 1.0
 
 

@@ -22,7 +22,8 @@ import os
 from pathlib import Path
 
 BUILD_BLOCKS = (64, 128, 256)
-SOLVE_SHAPES = [(b, p, u) for b in (128, 256) for p in (1, 2) for u in (2, 4, 8)]
+SOLVE_SHAPES = [(b, p, u) for b in (128, 256) for p in (1, 2) for u in (2, 4, 8)] + [(512, 1, 4), (1024, 1, 4)]
+DEFAULT_SOLVE = (1024, 1, 4)  # the library's shape when SphParams leaves it 0
 CACHE = Path(os.environ.get("WPSPH_AUTOTUNE_CACHE", Path.home() / ".cache" / "warpsph_b200" / "autotune.json"))
 
 
@@ -77,7 +78,8 @@ def autotune(scenes, params, warm=10, steps=20, use_cache=True, verbose=False) -
     # the build sweep ran the solve at the caller's shape (the library's
     # default where unset), so best_t is that shape's time: a solve shape must
     # beat it to replace it
-    best = (params.jacobi_block or 256, params.jacobi_ppt or 1, params.jacobi_unroll or 4)
+    best = (params.jacobi_block or DEFAULT_SOLVE[0], params.jacobi_ppt or DEFAULT_SOLVE[1],
+            params.jacobi_unroll or DEFAULT_SOLVE[2])
     for blk, ppt, unr in SOLVE_SHAPES:
         t = _time(scenes, params.replace(block_size=best_build, jacobi_block=blk, jacobi_ppt=ppt,
                                          jacobi_unroll=unr), warm, steps)

@@ -503,6 +503,8 @@ static JacobiKernel pick_jacobi(int T, int ppt, int unroll) {
   SPH_JACOBI_CASE(256, 2, 2)
   SPH_JACOBI_CASE(256, 2, 4)
   SPH_JACOBI_CASE(256, 2, 8)
+  SPH_JACOBI_CASE(512, 1, 4)
+  SPH_JACOBI_CASE(1024, 1, 4)
 #undef SPH_JACOBI_CASE
   return nullptr;
 }

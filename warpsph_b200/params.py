@@ -40,7 +40,7 @@ class SolverParams:
     device: int = 0
     block_size: int = 0           # neighbour build threads per block (0 = 128)
     timeout_ms: int = 2000
-    jacobi_block: int = 0         # pressure solve threads per block (0 = 256)
+    jacobi_block: int = 0         # pressure solve threads per block (0 = 1024)
     jacobi_ppt: int = 0           # particles per solve thread (0 = 1)
     jacobi_unroll: int = 0        # solve neighbour-loop unroll (0 = 4)
     move_boundary: bool = False   # boundary moves with its velocities (DYNAMIC_SCENE, main.py:20)
