@@ -75,10 +75,11 @@ struct Consts {
 // [fluid_off[s], fluid_off[s+1]), boundary slots [bound_off[s], ...), its own
 // grid, and global cell ids [cell_base[s], cell_base[s+1]): keys of different
 // scenes never mix, so the cell sort keeps every scene in its slot range and
-// neighbour searches never cross scenes.  Jacobi work is cut into chunks of at
-// most one solve block's worth of particles that never straddle scenes: chunks [chunk_off[s],
-// chunk_off[s+1]) belong to scene s.  A single scene is the case nscenes = 1.
-// A chunk is (threads per block) x (particles per thread) of the solve kernel.
+// neighbour searches never cross scenes.  Jacobi work is cut into warp-aligned
+// chunks of at most one solve block's worth of particles ((threads per block)
+// x (particles per thread)) that never straddle scenes, as many as the
+// persistent grid takes in whole rounds: chunks [chunk_off[s], chunk_off[s+1])
+// belong to scene s.  A single scene is the case nscenes = 1.
 constexpr int kMaxScenes = 256;
 
 struct SceneTable {
