@@ -274,7 +274,12 @@ __device__ __forceinline__ void jacobi_body(const JacobiArgs& a, const Tab& G) {
         es = 0.0;
         ec = 0;
       };
-      for (int ch = c_lo; ch < c_hi; ch += c_step) {
+      // with runs, pass B walks its run backwards: it starts on the chunk
+      // pass A just finished (its lists and records still cached), and the
+      // next pass A starts on the chunk pass B finished last
+      const int nb_ch = (c_hi - c_lo + c_step - 1) / c_step;
+      for (int t = 0; t < nb_ch; ++t) {
+        const int ch = runs ? c_hi - 1 - t : c_lo + t * c_step;
         const int s = __ldg(a.chunk_scene + ch);
         if (s != run) {
           if (run >= 0) flush();
